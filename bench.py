@@ -1,0 +1,347 @@
+"""Benchmark of the batched P-T-z flash on B200 (one JSON line on rank 0).
+
+Workload: 1,048,576 independent P-T-z points, nc = 3 (H2O/CO2/nC10), PR EOS,
+seeded synthetic mixture of roughly 40/40/20 % single/two/three-phase points
+(nonenone_b200.synth.flash_points).  A step is one flash of the whole batch.
+
+  value  flashes/s with inputs resident in HBM (CUDA events on the launching
+         stream, L2 flushed before every step and the flush left untimed)
+  e2e    the same through nz_flash_batch_host with pinned host buffers: the
+         host->device inputs and device->host results are inside the region
+  roofline  the flash kernel against the measured FP64 FMA peak of the box;
+         algorithmic FLOPs = executed EOS evaluations x F_eos(nc),
+         F_eos(nc) = 2 nc^2 + 13 nc + 50
+  cpu_baseline  the reference's own FP64 flash (oracle/_ref, compiled from the
+         reference tree) on a bounded sample, all host threads
+
+--impl reference times that reference CPU flash alone (rank 0; other ranks
+exit).  With --gpus N under torchrun every rank flashes its own batch (weak
+scaling, no collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell flash+Jacobian evals/s (mixed vs FP64 GPU, 1e-10 fug. tol); p50/p99 latency"
+UNIT = "flash evals/s"
+N_POINTS = 1 << 20
+NC = 3
+
+
+def f_eos(nc: int) -> int:
+    return 2 * nc * nc + 13 * nc + 50
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock / throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.path is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(fluid, P, T, z, seconds_target: float = 15.0):
+    """The reference's FP64 flash on host cores over a bounded sample."""
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    # size the sample from a quick single-thread probe of the same workload
+    probe = 256
+    t0 = time.perf_counter()
+    ref.flash_batch(fluid, P[:probe], T[:probe], z[:, :probe], threads=1)
+    per_point = (time.perf_counter() - t0) / probe
+    m = int(min(P.shape[0], max(threads * 64, seconds_target * threads / max(per_point, 1e-7))))
+    t0 = time.perf_counter()
+    ref.flash_batch(fluid, P[:m], T[:m], z[:, :m], threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": m / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"first {m} of the {P.shape[0]} workload points (the seeded mixture is "
+                      f"shuffled, so the sample has the workload's label mix); "
+                      f"{threads} threads, one CubicThreePhaseFlash each; {dt:.1f} s",
+            "single_core_us_per_flash": per_point * 1e6}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from nonenone_b200 import synth
+    from nonenone_b200.fluids import make_fluid
+    from oracle import ref
+    fluid = make_fluid()
+    P, T, z = synth.flash_points(N_POINTS, seed=1)
+    threads = os.cpu_count() or 1
+    # each step is a bounded, rotating sample of the workload sized so the
+    # whole --steps/--warmup run stays within a few minutes
+    probe = 256
+    t0 = time.perf_counter()
+    ref.flash_batch(fluid, P[:probe], T[:probe], z[:, :probe], threads=1)
+    per_point = (time.perf_counter() - t0) / probe
+    m = int(min(N_POINTS, max(threads * 32, 8.0 * threads / max(per_point, 1e-7))))
+    off = 0
+    for _ in range(args.warmup):
+        sl = slice(off, off + m)
+        ref.flash_batch(fluid, P[sl], T[sl], z[:, sl], threads=threads)
+        off = (off + m) % (N_POINTS - m)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sl = slice(off, off + m)
+        ref.flash_batch(fluid, P[sl], T[sl], z[:, sl], threads=threads)
+        off = (off + m) % (N_POINTS - m)
+    dt = time.perf_counter() - t0
+    rate = m * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "batched P-T-z flash, 1,048,576 points, nc=3 H2O/CO2/nC10, PR",
+                   "points_per_step": m, "eos": "PR", "nc": NC},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{m} workload points per step, {threads} threads"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import torch
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from nonenone_b200 import abi, synth
+    from nonenone_b200.fluids import make_fluid
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    from nonenone_b200.lib import load
+    import ctypes as C
+
+    fluid = make_fluid()
+    precision = abi.PRECISION_MIXED if args.precision == "mixed" else abi.PRECISION_FP64
+    fl = CubicThreePhaseFlash(fluid, device=local)
+    P, T, z = synth.flash_points(N_POINTS, seed=1 + rank)
+    dev = fl.device
+    Pd = torch.tensor(P, device=dev)
+    Td = torch.tensor(T, device=dev)
+    zd = torch.tensor(z, device=dev)
+    out = fl.allocate(N_POINTS)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # 256 MiB > 126 MB L2
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step():
+        fl.flash(Pd, Td, zd, out=out, precision=precision, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    evals = []
+    with ClockSampler(local) as clocks:
+        barrier()
+        for k in range(args.steps):
+            flush.zero_()                      # untimed: L2 holds no input of the step
+            events[k][0].record(stream)
+            step()
+            events[k][1].record(stream)
+            torch.cuda.synchronize()
+            evals.append(fl.eos_eval_count())
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    total_ms = sum(step_ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = N_POINTS * world * args.steps / (total_ms * 1e-3)
+
+    # --- e2e: host buffers through the host entry point -----------------------
+    Ph = torch.from_numpy(P).pin_memory()
+    Th = torch.from_numpy(T).pin_memory()
+    zh = torch.from_numpy(z).pin_memory()
+    nc = NC
+    host_out = {
+        "presence": torch.empty(N_POINTS, dtype=torch.uint8).pin_memory(),
+        "status": torch.empty(N_POINTS, dtype=torch.uint8).pin_memory(),
+        "beta": torch.empty(3, N_POINTS, dtype=torch.float64).pin_memory(),
+        "saturation": torch.empty(3, N_POINTS, dtype=torch.float64).pin_memory(),
+        "composition": torch.empty(3, nc, N_POINTS, dtype=torch.float64).pin_memory(),
+        "compressibility": torch.empty(3, N_POINTS, dtype=torch.float64).pin_memory(),
+        "molar_density": torch.empty(3, N_POINTS, dtype=torch.float64).pin_memory(),
+        "k_gas_oil": torch.empty(nc, N_POINTS, dtype=torch.float64).pin_memory(),
+        "k_water_oil": torch.empty(nc, N_POINTS, dtype=torch.float64).pin_memory(),
+        "iterations": torch.empty(N_POINTS, dtype=torch.int32).pin_memory(),
+    }
+    lib = load()
+    fo = abi.FlashOut(*[host_out[k].data_ptr() for k, _ in abi.FlashOut._fields_])
+    h2d = N_POINTS * (2 + nc) * 8
+    d2h = sum(t.numel() * t.element_size() for t in host_out.values())
+
+    def e2e_step():
+        rc = lib.nz_flash_batch_host(fl.handle, N_POINTS, C.c_void_p(Ph.data_ptr()),
+                                     C.c_void_p(Th.data_ptr()), C.c_void_p(zh.data_ptr()), None,
+                                     C.byref(fo), precision)
+        if rc != 0:
+            raise RuntimeError(lib.nz_last_error().decode())
+
+    e2e_step()
+    barrier()
+    e2e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = N_POINTS * world * e2e_steps / e2e_s
+
+    # --- roofline of the flash kernel ------------------------------------------
+    fp64 = C.c_double()
+    fp32 = C.c_double()
+    lib.nz_diag_fma_peak(local, C.byref(fp64), C.byref(fp32))
+    kernel_s = np.mean(step_ms) * 1e-3
+    flops = np.mean(evals) * f_eos(nc)
+    achieved = flops / kernel_s / 1e12
+    peak = fp64.value if precision == abi.PRECISION_FP64 else fp32.value
+    status = out["status"].cpu().numpy()
+    presence = out["presence"].cpu().numpy()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                from oracle import ref
+                if ref.available():
+                    cpu = cpu_reference_rate(fluid, P, T, z)
+            except Exception as ex:   # the baseline must not mask the GPU number
+                cpu = {"value": None, "error": str(ex)}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == abi.PRECISION_FP64 else "f32+f64",
+            "data": "synthetic (seeded mixture, nonenone_b200.synth.flash_points)",
+            "config": {"workload": "batched P-T-z flash, 1,048,576 points per GPU, nc=3 "
+                                   "H2O/CO2/nC10, PR EOS",
+                       "points_per_gpu": N_POINTS, "eos": "PR", "nc": NC,
+                       "precision": args.precision, "l2": "flushed (256 MiB write) before each step, untimed",
+                       "label_mix": {"single": float(np.isin(presence, [1, 2, 4]).mean()),
+                                     "two": float(np.isin(presence, [3, 5, 6]).mean()),
+                                     "three": float((presence == 7).mean()),
+                                     "failed": float((status != 0).mean())}},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "entry_point": "nz_flash_batch_host"},
+            "roofline": {"bound": "fp64" if precision == abi.PRECISION_FP64 else "fp32",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "peak_source": "measured on this GPU by nz_diag_fma_peak (FMA chains); "
+                                        "not in MEASURED_PEAKS.json",
+                         "flops_per_launch": flops,
+                         "eos_evals_per_flash": float(np.mean(evals) / N_POINTS),
+                         "kernel": "flashKernel<3>"},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "fp32_fma_peak_tflops": fp32.value,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nz", choices=["nz", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

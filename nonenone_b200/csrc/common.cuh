@@ -1,0 +1,62 @@
+// common.cuh -- shared host-side definitions of the CUDA library.
+#pragma once
+
+#include "../../include/nonenone_b200.h"
+#include "eos.cuh"
+
+#include <cstdarg>
+#include <cuda_runtime.h>
+
+namespace nz
+{
+
+constexpr int kFlashBlock = 128;
+
+int setError(int code, const char *fmt, ...);
+int cudaFail(cudaError_t e, const char *what);
+
+inline bool ncSupported(int nc) { return nc == 3 || nc == 4 || nc == 5 || nc == 6 || nc == 8; }
+
+} // namespace nz
+
+// The opaque context behind nz_ctx*.
+struct nz_ctx
+{
+    int device{0};
+    nz_fluid_desc desc{};
+    nz_flash_options options{};
+    nz::FluidDev fluid{};
+    unsigned long long *evalCounter{nullptr};   // EOS evaluations of the last flash batch
+    cudaStream_t ownStream{nullptr};
+
+    cudaStream_t hostStream()
+    {
+        if (!ownStream)
+            cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking);
+        return ownStream;
+    }
+};
+
+namespace nz
+{
+int launchMixedFlash(nz_ctx *ctx, int64_t n, const double *P, const double *T, const double *z,
+                     const double *sal, const nz_flash_out &out, cudaStream_t st);
+}
+
+// Runtime nc -> compile-time NC dispatch over the instantiated component counts.
+#define DISPATCH_NC(ncv, fn, ...)                                                  \
+    do                                                                             \
+    {                                                                              \
+        int _rc = NZ_ERR_UNSUPPORTED;                                              \
+        switch (ncv)                                                               \
+        {                                                                          \
+        case 3: _rc = fn<3>(__VA_ARGS__); break;                                   \
+        case 4: _rc = fn<4>(__VA_ARGS__); break;                                   \
+        case 5: _rc = fn<5>(__VA_ARGS__); break;                                   \
+        case 6: _rc = fn<6>(__VA_ARGS__); break;                                   \
+        case 8: _rc = fn<8>(__VA_ARGS__); break;                                   \
+        default: return nz::setError(NZ_ERR_UNSUPPORTED, "nc=%d not compiled", int(ncv)); \
+        }                                                                          \
+        if (_rc != 0)                                                              \
+            return _rc;                                                            \
+    } while (0)

@@ -1,0 +1,2677 @@
+// flash.cuh -- device three-phase P-T-z flash, one thread per point, FP64.
+//
+// Restates the reference's CubicThreePhaseFlash
+// (models/include/natural/thermo/three_phase_flash.hpp and
+//  thermo/detail/three_phase_flash_{core,nonlinear,restricted,allocation,
+//  canonicalization,stability}.inc) decision for decision: the same
+// iteration caps, tolerances, finite-difference Newton steps, line searches,
+// seed lists, canonicalisation passes and fail-only recovery order.  Line
+// references below are to those files.
+//
+// Differences by design:
+//  * exceptions become an error code in `err`; the flash then returns with
+//    that status (the reference aborts the call with the exception);
+//  * the SSI steps of the TPD trial reuse the fugacity coefficients of the
+//    residual evaluation at the same composition (the reference evaluates
+//    the EOS twice there; the EOS is deterministic so the values are equal);
+//  * the Soreide-Whitson exact-mass allocation recovery
+//    (three_phase_flash_allocation.inc:609-700) is not carried: a point that
+//    reaches it returns NZ_FLASH_NOT_PORTED.
+#pragma once
+
+#include "eos.cuh"
+
+namespace nz
+{
+
+template <int NC>
+struct Result
+{
+    bool converged;
+    int iterations;
+    uint8_t presence;
+    double beta[3];
+    double sat[3];
+    double x[3][NC];
+    double Z[3];
+    double rho[3];
+    double Kg[NC];
+    double Kw[NC];
+
+    __device__ void init()
+    {
+        converged = false;
+        iterations = 0;
+        presence = ALL_BITS;
+        beta[0] = 1.0; beta[1] = 0.0; beta[2] = 0.0;
+        sat[0] = 1.0; sat[1] = 0.0; sat[2] = 0.0;
+        Z[0] = 1.0; Z[1] = 1.0; Z[2] = 1.0;
+        rho[0] = 0.0; rho[1] = 0.0; rho[2] = 0.0;
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                x[p][i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            Kg[i] = 0.0;
+            Kw[i] = 0.0;
+        }
+    }
+};
+
+template <int NC>
+struct StabilityResult
+{
+    bool stable;
+    bool valid;
+    uint8_t tested;
+    bool unstable[3];
+    double incipient[3][NC];
+    double trialSum[3];
+};
+
+template <int NC>
+struct Trial
+{
+    bool valid;
+    bool trivial;
+    double sum;
+    double x[NC];
+};
+
+template <int NC>
+struct StabilityResidual
+{
+    bool valid;
+    double norm;
+    double sum;
+    double x[NC];
+    double residual[NC];
+    double phi[NC];
+};
+
+template <int NC>
+struct TwoPhaseLogKState
+{
+    bool valid;
+    double norm;
+    double residual[NC];
+    Result<NC> result;
+};
+
+template <int NC>
+struct ThreePhaseLogKState
+{
+    bool valid;
+    double norm;
+    double residual[2 * NC];
+    Result<NC> result;
+};
+
+// ---- small helpers ---------------------------------------------------------
+__device__ __forceinline__ int firstActive(uint8_t b)
+{
+    return (b & OIL_BIT) ? OIL : ((b & GAS_BIT) ? GAS : WATER);
+}
+
+__device__ __forceinline__ void activePair(uint8_t b, int &first, int &second)
+{
+    int n = 0;
+    first = OIL;
+    second = GAS;
+    for (int p = 0; p < 3; ++p)
+    {
+        if (b & bitOf(p))
+        {
+            if (n == 0) first = p;
+            else if (n == 1) second = p;
+            ++n;
+        }
+    }
+}
+
+// Dense Gaussian elimination with partial pivoting (stability.inc:98-146).
+template <int M>
+__device__ bool solveDense(double (&m)[M][M], double (&rhs)[M], double (&sol)[M])
+{
+#pragma unroll 1
+    for (int k = 0; k < M; ++k)
+        sol[k] = 0.0;
+#pragma unroll 1
+    for (int col = 0; col < M; ++col)
+    {
+        int pivot = col;
+#pragma unroll 1
+        for (int row = col + 1; row < M; ++row)
+            if (fabs(m[row][col]) > fabs(m[pivot][col]))
+                pivot = row;
+        if (!(fabs(m[pivot][col]) > 1.0e-13))
+            return false;
+        if (pivot != col)
+        {
+#pragma unroll 1
+            for (int j = 0; j < M; ++j)
+            {
+                const double t = m[pivot][j];
+                m[pivot][j] = m[col][j];
+                m[col][j] = t;
+            }
+            const double t = rhs[pivot];
+            rhs[pivot] = rhs[col];
+            rhs[col] = t;
+        }
+#pragma unroll 1
+        for (int row = col + 1; row < M; ++row)
+        {
+            const double factor = m[row][col] / m[col][col];
+            if (!isfinite(factor))
+                return false;
+#pragma unroll 1
+            for (int j = col; j < M; ++j)
+                m[row][j] -= factor * m[col][j];
+            rhs[row] -= factor * rhs[col];
+        }
+    }
+#pragma unroll 1
+    for (int rev = 0; rev < M; ++rev)
+    {
+        const int row = M - 1 - rev;
+        double value = rhs[row];
+#pragma unroll 1
+        for (int j = row + 1; j < M; ++j)
+            value -= m[row][j] * sol[j];
+        if (!(fabs(m[row][row]) > 1.0e-13))
+            return false;
+        sol[row] = value / m[row][row];
+        if (!isfinite(sol[row]))
+            return false;
+    }
+    return true;
+}
+
+// The SW role permutations (core.inc:37-45).
+__device__ __forceinline__ void swRolePermutation(int k, int (&roles)[3])
+{
+    const int table[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    roles[0] = table[k][0];
+    roles[1] = table[k][1];
+    roles[2] = table[k][2];
+}
+
+// ============================================================================
+template <int NC>
+struct Solver
+{
+    const FluidDev *F;
+    double salinity;
+    int roles[3];
+    bool permutationSearch;
+    bool continuation;
+    int err;
+    unsigned long long evals;
+    // cubic parameter cache (core.inc:71-99)
+    bool cacheValid;
+    double cacheP, cacheT;
+    MixParams<NC> nonAq;
+    MixParams<NC> aq;
+
+    __device__ void setup(const FluidDev *fluid, double s)
+    {
+        F = fluid;
+        salinity = s;
+        roles[0] = OIL; roles[1] = GAS; roles[2] = WATER;
+        permutationSearch = true;
+        continuation = true;
+        err = ERR_NONE;
+        evals = 0;
+        cacheValid = false;
+        cacheP = cacheT = 0.0;
+    }
+
+    __device__ const FlashOpts &O() const { return F->opt; }
+    __device__ bool sw() const { return F->eosModel == EOS_SW; }
+
+    __device__ void fail(int code)
+    {
+        if (err == ERR_NONE)
+            err = code;
+    }
+
+    // ---------------------------------------------------------------- core --
+    __device__ int thermodynamicRole(int slot) const { return sw() ? roles[slot] : slot; }
+
+    __device__ void ensureCache(double P, double T)
+    {
+        if (cacheValid && cacheP == P && cacheT == T)
+            return;
+        mixingParameters<NC>(*F, P, T, salinity, false, nonAq);
+        if (sw())
+            mixingParameters<NC>(*F, P, T, salinity, true, aq);
+        cacheP = P;
+        cacheT = T;
+        cacheValid = true;
+    }
+
+    // phaseResultForThermodynamicRole_ (core.inc:101-126)
+    __device__ __noinline__ double phaseForRole(int role, double P, double T, const double *x, double *phi)
+    {
+        ensureCache(P, T);
+        const MixParams<NC> &p = (role == WATER && sw()) ? aq : nonAq;
+        PhaseMix<NC> m;
+        phaseMixing<NC>(x, p, m);
+        ++evals;
+        const double Z = selectCubicRoot(m.A, m.B, F->m1, F->m2, role == GAS);
+        if (!isfinite(Z) || !fugacityCoefficients<NC>(x, p, m, Z, F->m1, F->m2, phi))
+        {
+            fail(ERR_EOS);
+            const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                phi[i] = nan;
+            return nan;
+        }
+        return Z;
+    }
+
+    __device__ double phase(int slot, double P, double T, const double *x, double *phi)
+    {
+        return phaseForRole(thermodynamicRole(slot), P, T, x, phi);
+    }
+
+    __device__ bool validatePT(double P, double T)
+    {
+        if (!(P > 0.0) || !isfinite(P) || !(T > 0.0) || !isfinite(T))
+        {
+            fail(ERR_BAD_INPUT);
+            return false;
+        }
+        return true;
+    }
+
+    // normalize_ (core.inc:136-149)
+    __device__ void normalize(double *x)
+    {
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            if (!isfinite(x[i]))
+                fail(ERR_BAD_INPUT);
+            x[i] = smax(x[i], O().floor);
+            sum += x[i];
+        }
+        if (!(sum > 0.0))
+            fail(ERR_BAD_INPUT);
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            x[i] /= sum;
+    }
+
+    // wilsonGasOilK_ (core.inc:152-165)
+    __device__ void wilsonK(double P, double T, double *K) const
+    {
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double lnK = log(F->pc[i] / P) + 5.373 * (1.0 + F->omega[i]) * (1.0 - F->tc[i] / T);
+            K[i] = sclamp(exp(lnK), 1.0e-30, 1.0e30);
+        }
+    }
+
+    // initialWaterOilK_ (core.inc:168-176)
+    __device__ void initialWaterK(double *K) const
+    {
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            K[i] = 0.05;
+        K[F->water >= 0 ? F->water : NC - 1] = 50.0;
+    }
+
+    __device__ uint8_t presenceFromFractions(const double *beta) const
+    {
+        uint8_t b = 0;
+        for (int p = 0; p < 3; ++p)
+            if (beta[p] > O().betaTol)
+                b |= uint8_t(bitOf(p));
+        return b;
+    }
+
+    // ------------------------------------------------------- Rachford-Rice --
+    // residual/Jacobian of the three-phase RR (nonlinear.inc:30-58)
+    __device__ double rr3Norm(const double *z, const double *kg, const double *kw, double cg, double cw,
+                              double &fg, double &fw, double &jgg, double &jww, double &jgw) const
+    {
+        const double inf = __longlong_as_double(0x7ff0000000000000LL);
+        if (!(cg > 0.0) || !(cw > 0.0) || !(cg + cw < 1.0))
+            return inf;
+        fg = 0.0; fw = 0.0; jgg = 0.0; jww = 0.0; jgw = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double ag = kg[i] - 1.0;
+            const double aw = kw[i] - 1.0;
+            const double co = 1.0 - cg - cw;
+            const double D = co + cg * kg[i] + cw * kw[i];
+            if (!(D > 1.0e-12) || !isfinite(D))
+                return inf;
+            fg += z[i] * ag / D;
+            fw += z[i] * aw / D;
+            const double invD2 = z[i] / (D * D);
+            jgg -= invD2 * ag * ag;
+            jww -= invD2 * aw * aw;
+            jgw -= invD2 * ag * aw;
+        }
+        return smax(fabs(fg), fabs(fw));
+    }
+
+    // solveRr3_ (nonlinear.inc:8-96)
+    __device__ bool rr3(const double *z, const double *kg, const double *kw, double initBg, double initBw,
+                        double &outBg, double &outBw) const
+    {
+        double bg = sclamp(initBg, 1.0e-4, 0.8);
+        double bw = sclamp(initBw, 1.0e-4, 0.8);
+        if (bg + bw >= 0.95)
+        {
+            const double scale = 0.8 / (bg + bw);
+            bg *= scale;
+            bw *= scale;
+        }
+#pragma unroll 1
+        for (int it = 0; it < O().maxRr; ++it)
+        {
+            double fg, fw, jgg, jww, jgw;
+            const double norm = rr3Norm(z, kg, kw, bg, bw, fg, fw, jgg, jww, jgw);
+            if (!isfinite(norm))
+                return false;
+            if (norm < O().rrTol)
+            {
+                outBg = bg;
+                outBw = bw;
+                return true;
+            }
+            const double det = jgg * jww - jgw * jgw;
+            if (fabs(det) < 1.0e-24 || !isfinite(det))
+                return false;
+            const double dbg = (-fg * jww + fw * jgw) / det;
+            const double dbw = (-fw * jgg + fg * jgw) / det;
+            double lambda = 1.0;
+            bool accepted = false;
+#pragma unroll 1
+            for (int ls = 0; ls < 40; ++ls)
+            {
+                const double cg = bg + lambda * dbg;
+                const double cw = bw + lambda * dbw;
+                double a, b, c, d, e;
+                const double cn = rr3Norm(z, kg, kw, cg, cw, a, b, c, d, e);
+                if (isfinite(cn) && cn < norm)
+                {
+                    bg = cg;
+                    bw = cw;
+                    accepted = true;
+                    break;
+                }
+                lambda *= 0.5;
+            }
+            if (!accepted)
+                return false;
+        }
+        return false;
+    }
+
+    // solveRr3Robust_ (nonlinear.inc:98-127)
+    __device__ bool rr3Robust(const double *z, const double *kg, const double *kw, double pg, double pw,
+                              double &bg, double &bw) const
+    {
+        const double guesses[17][2] = {
+            {pg, pw}, {0.333, 0.333}, {0.50, 1.0e-4}, {1.0e-4, 0.50}, {0.80, 1.0e-4},
+            {1.0e-4, 0.80}, {0.20, 0.20}, {0.60, 0.20}, {0.20, 0.60}, {0.05, 0.05},
+            {0.90, 0.01}, {0.95, 1.0e-4}, {0.98, 1.0e-4}, {1.0e-4, 0.95}, {1.0e-4, 0.98},
+            {0.01, 0.90}, {0.45, 0.45}};
+#pragma unroll 1
+        for (int g = 0; g < 17; ++g)
+            if (rr3(z, kg, kw, guesses[g][0], guesses[g][1], bg, bw))
+                return true;
+        return false;
+    }
+
+    // solveRr2_ (nonlinear.inc:129-187)
+    __device__ double rr2Eval(const double *z, const double *K, double beta, double &df) const
+    {
+        double f = 0.0;
+        df = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double a = K[i] - 1.0;
+            const double D = (1.0 - beta) + beta * K[i];
+            if (!(D > 1.0e-300) || !isfinite(D))
+                return __longlong_as_double(0x7ff8000000000000LL);
+            f += z[i] * a / D;
+            df -= z[i] * a * a / (D * D);
+        }
+        return f;
+    }
+
+    __device__ bool rr2(const double *z, const double *K, double initialBeta, double &out) const
+    {
+        double d0;
+        const double f0 = rr2Eval(z, K, 0.0, d0);
+        const double f1 = rr2Eval(z, K, 1.0, d0);
+        if (!isfinite(f0) || !isfinite(f1))
+            return false;
+        if (f0 <= 0.0)
+        {
+            out = 0.0;
+            return true;
+        }
+        if (f1 >= 0.0)
+        {
+            out = 1.0;
+            return true;
+        }
+        double lower = 0.0, upper = 1.0;
+        double beta = sclamp(initialBeta, lower, upper);
+#pragma unroll 1
+        for (int it = 0; it < O().maxRr; ++it)
+        {
+            double df;
+            const double f = rr2Eval(z, K, beta, df);
+            if (!isfinite(f) || !isfinite(df))
+                return false;
+            if (fabs(f) < O().rrTol)
+            {
+                out = beta;
+                return true;
+            }
+            if (f > 0.0) lower = beta; else upper = beta;
+            double candidate = beta;
+            if (fabs(df) > 1.0e-24)
+                candidate = beta - f / df;
+            if (!isfinite(candidate) || candidate <= lower || candidate >= upper)
+                candidate = 0.5 * (lower + upper);
+            beta = candidate;
+        }
+        return false;
+    }
+
+    // ----------------------------------------------------- result helpers --
+    // deriveReferenceK_ (restricted.inc:414-423)
+    __device__ void deriveReferenceK(Result<NC> &r) const
+    {
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double xo = smax(r.x[0][i], O().floor);
+            r.Kg[i] = r.x[1][i] / xo;
+            r.Kw[i] = r.x[2][i] / xo;
+        }
+    }
+
+    // updateSaturationsFromMoles (three_phase_flash.hpp:527-575).  No aqueous
+    // volume closure is configured, so every Water composition is admissible.
+    __device__ void updateSaturations(double P, double T, Result<NC> &r)
+    {
+        double volumeSum = 0.0;
+        double volume[3] = {0.0, 0.0, 0.0};
+        for (int p = 0; p < 3; ++p)
+        {
+            if (!(r.presence & bitOf(p)))
+            {
+                r.beta[p] = 0.0;
+                r.sat[p] = 0.0;
+                r.rho[p] = 0.0;
+                continue;
+            }
+            const double Z = r.Z[p];
+            if (!(Z > 0.0))
+            {
+                fail(ERR_EOS);
+                return;
+            }
+            const double rhoM = molarDensity(P, T, Z);
+            r.rho[p] = rhoM;
+            volume[p] = smax(r.beta[p], 0.0) / rhoM;
+            volumeSum += volume[p];
+        }
+        if (!(volumeSum > 0.0))
+        {
+            fail(ERR_EOS);
+            return;
+        }
+        for (int p = 0; p < 3; ++p)
+            r.sat[p] = volume[p] / volumeSum;
+    }
+
+    // singlePhaseResult_ (restricted.inc:425-447)
+    __device__ void singlePhaseResult(double P, double T, const double *z, uint8_t active, Result<NC> &r)
+    {
+        r.init();
+        r.converged = true;
+        r.presence = active;
+        r.beta[0] = r.beta[1] = r.beta[2] = 0.0;
+        const int p = firstActive(active);
+        r.beta[p] = 1.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            r.x[p][i] = z[i];
+        for (int q = 0; q < 3; ++q)
+            if (!(active & bitOf(q)))
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    r.x[q][i] = z[i];
+        double phi[NC];
+        r.Z[p] = phase(p, P, T, z, phi);
+        deriveReferenceK(r);
+        updateSaturations(P, T, r);
+    }
+
+    // waterIsDominant_ (canonicalization.inc:68-85)
+    __device__ bool waterIsDominant(const double *x) const
+    {
+        if (F->water < 0)
+            return false;
+        double largestOther = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            if (i != F->water)
+                largestOther = smax(largestOther, x[i]);
+        return x[F->water] >= largestOther;
+    }
+
+    // chooseSinglePhase_ (restricted.inc:449-478)
+    __device__ uint8_t chooseSinglePhase(double P, double T, const double *z)
+    {
+        double phi[NC];
+        double g[3];
+        for (int p = 0; p < 3; ++p)
+        {
+            phase(p, P, T, z, phi);
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                s += z[i] * log(smax(phi[i], 1.0e-300));
+            g[p] = s;
+        }
+        const double go = g[0], gg = g[1], gw = g[2];
+        const double tie = 1.0e-10;
+        if (gg + tie < go && gg + tie < gw)
+            return GAS_BIT;
+        if (gw + tie < go && gw + tie < gg)
+            return WATER_BIT;
+        if (waterIsDominant(z) && fabs(gw - go) <= tie)
+            return WATER_BIT;
+        if (gg + tie < go)
+            return GAS_BIT;
+        return OIL_BIT;
+    }
+
+    // dimensionlessGibbs_ (restricted.inc:480-505); the public slot is the role.
+    __device__ double dimensionlessGibbs(double P, double T, const Result<NC> &r)
+    {
+        double g = 0.0;
+        double phi[NC];
+        for (int p = 0; p < 3; ++p)
+        {
+            const double beta = r.beta[p];
+            if (!(beta > O().betaTol))
+                continue;
+            phaseForRole(p, P, T, r.x[p], phi);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+            {
+                const double xi = smax(r.x[p][i], O().floor);
+                const double ph = smax(phi[i], 1.0e-300);
+                g += beta * r.x[p][i] * (log(xi) + log(ph));
+            }
+        }
+        return g;
+    }
+
+    __device__ void swapSlots(Result<NC> &r, int a, int b) const
+    {
+        if (a == b)
+            return;
+        double t;
+        t = r.beta[a]; r.beta[a] = r.beta[b]; r.beta[b] = t;
+        t = r.sat[a]; r.sat[a] = r.sat[b]; r.sat[b] = t;
+        t = r.Z[a]; r.Z[a] = r.Z[b]; r.Z[b] = t;
+        t = r.rho[a]; r.rho[a] = r.rho[b]; r.rho[b] = t;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            t = r.x[a][i]; r.x[a][i] = r.x[b][i]; r.x[b][i] = t;
+        }
+    }
+
+    // ------------------------------------------------------- pair seeds ----
+    // pairInitialK_ (nonlinear.inc:515-623)
+    __device__ void pairInitialK(int first, int second, double P, double T, const double *z, double *K)
+    {
+        if (sw() && (first == WATER || second == WATER))
+        {
+            const int water = F->water >= 0 ? F->water : NC - 1;
+            double seeds[2][NC];
+            const int which[2] = {first, second};
+            for (int s = 0; s < 2; ++s)
+            {
+                double *seed = seeds[s];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    seed[i] = z[i];
+                if (which[s] == WATER)
+                {
+                    double nonWater = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                    {
+                        if (i == water) continue;
+                        seed[i] = smax(z[i], O().floor);
+                        nonWater += seed[i];
+                    }
+                    const double dissolved = 0.02;
+                    if (nonWater > 0.0)
+#pragma unroll
+                        for (int i = 0; i < NC; ++i)
+                            if (i != water)
+                                seed[i] *= dissolved / nonWater;
+                    seed[water] = 1.0 - dissolved;
+                }
+                else
+                {
+                    const double waterSeed = 0.01;
+                    double nonWater = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        if (i != water)
+                            nonWater += smax(z[i], O().floor);
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                    {
+                        if (i == water)
+                            seed[i] = waterSeed;
+                        else
+                            seed[i] = nonWater > 0.0
+                                ? (1.0 - waterSeed) * smax(z[i], O().floor) / nonWater
+                                : (1.0 - waterSeed) / double(NC - 1 > 1 ? NC - 1 : 1);
+                    }
+                }
+                normalize(seed);
+            }
+            double phiA[NC], phiB[NC];
+            phase(first, P, T, seeds[0], phiA);
+            phase(second, P, T, seeds[1], phiB);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                K[i] = sclamp(smax(phiA[i], 1.0e-300) / smax(phiB[i], 1.0e-300), 1.0e-100, 1.0e100);
+            return;
+        }
+        double kg[NC], kw[NC];
+        wilsonK(P, T, kg);
+        initialWaterK(kw);
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double rs = second == OIL ? 1.0 : (second == GAS ? kg[i] : kw[i]);
+            const double rf = first == OIL ? 1.0 : (first == GAS ? kg[i] : kw[i]);
+            K[i] = rs / rf;
+        }
+    }
+
+    // --------------------------------------------------------- two-phase ---
+    // evaluateTwoPhaseLogK_ (restricted.inc:71-134)
+    __device__ __noinline__ void evalTwo(double P, double T, const double *z, int first, int second,
+                                         const double *logK, double preferredSecond,
+                                         TwoPhaseLogKState<NC> &s)
+    {
+        s.valid = false;
+        s.norm = __longlong_as_double(0x7ff0000000000000LL);
+        s.result.init();
+        double K[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            K[i] = exp(sclamp(logK[i], -230.0, 230.0));
+        double bS;
+        if (!rr2(z, K, preferredSecond, bS))
+            return;
+        const double bF = 1.0 - bS;
+        double a[NC], b[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double D = (1.0 - bS) + bS * K[i];
+            if (!(D > 0.0) || !isfinite(D))
+                return;
+            a[i] = z[i] / D;
+            b[i] = K[i] * a[i];
+        }
+        normalize(a);
+        normalize(b);
+        double phiA[NC], phiB[NC];
+        const double ZA = phase(first, P, T, a, phiA);
+        const double ZB = phase(second, P, T, b, phiB);
+        s.norm = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double pa = smax(phiA[i], 1.0e-300);
+            const double pb = smax(phiB[i], 1.0e-300);
+            s.residual[i] = logK[i] - log(pa / pb);
+            s.norm = smax(s.norm, fabs(s.residual[i]));
+        }
+        Result<NC> &r = s.result;
+        r.presence = uint8_t(bitOf(first) | bitOf(second));
+        r.beta[0] = r.beta[1] = r.beta[2] = 0.0;
+        r.beta[first] = bF;
+        r.beta[second] = bS;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            r.x[first][i] = a[i];
+            r.x[second][i] = b[i];
+        }
+        r.Z[first] = ZA;
+        r.Z[second] = ZB;
+        for (int p = 0; p < 3; ++p)
+            if (!(r.presence & bitOf(p)))
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    r.x[p][i] = z[i];
+        s.valid = isfinite(s.norm);
+    }
+
+    // one damped SSI step of flashTwo_ (restricted.inc:155-208)
+    __device__ bool twoSsiStep(double P, double T, const double *z, int first, int second, double *K,
+                               double &betaSecond, int &totalIterations, Result<NC> &r)
+    {
+        double bS;
+        if (!rr2(z, K, betaSecond, bS))
+            return false;
+        betaSecond = bS;
+        const double bF = 1.0 - bS;
+        double a[NC], b[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double D = (1.0 - bS) + bS * K[i];
+            if (!(D > 0.0) || !isfinite(D))
+                return false;
+            a[i] = z[i] / D;
+            b[i] = K[i] * a[i];
+        }
+        normalize(a);
+        normalize(b);
+        double phiA[NC], phiB[NC];
+        const double ZA = phase(first, P, T, a, phiA);
+        const double ZB = phase(second, P, T, b, phiB);
+        double maxResidual = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double target = smax(phiA[i], 1.0e-300) / smax(phiB[i], 1.0e-300);
+            const double d = sclamp(log(target / K[i]), -O().logKLimit, O().logKLimit);
+            maxResidual = smax(maxResidual, fabs(d));
+            K[i] *= exp(0.6 * d);
+            K[i] = sclamp(K[i], 1.0e-100, 1.0e100);
+        }
+        ++totalIterations;
+        r.iterations = totalIterations;
+        r.beta[0] = r.beta[1] = r.beta[2] = 0.0;
+        r.beta[first] = bF;
+        r.beta[second] = bS;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            r.x[first][i] = a[i];
+            r.x[second][i] = b[i];
+        }
+        r.Z[first] = ZA;
+        r.Z[second] = ZB;
+        for (int p = 0; p < 3; ++p)
+            if (!(r.presence & bitOf(p)))
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    r.x[p][i] = z[i];
+        if (maxResidual < O().fugacityTol)
+        {
+            r.converged = true;
+            r.presence = presenceFromFractions(r.beta);
+            deriveReferenceK(r);
+            updateSaturations(P, T, r);
+        }
+        return true;
+    }
+
+    // flashTwo_ (restricted.inc:136-327)
+    __device__ __noinline__ void flashTwo(double P, double T, const double *z, int first, int second,
+                                          const double *Kin, Result<NC> &r)
+    {
+        r.init();
+        r.presence = uint8_t(bitOf(first) | bitOf(second));
+        double K[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            K[i] = sclamp(Kin[i], 1.0e-100, 1.0e100);
+        double betaSecond = 0.5;
+        int total = 0;
+        const int ssiSteps = min(O().maxIterations, max(O().twoSsi, 0));
+#pragma unroll 1
+        for (int it = 0; it < ssiSteps; ++it)
+        {
+            if (!twoSsiStep(P, T, z, first, second, K, betaSecond, total, r))
+                return;
+            if (r.converged || err)
+                return;
+        }
+        double logK[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            logK[i] = log(K[i]);
+
+        TwoPhaseLogKState<NC> base, probe;
+#pragma unroll 1
+        for (int it = 0; it < O().twoNewton; ++it)
+        {
+            evalTwo(P, T, z, first, second, logK, betaSecond, base);
+            if (!base.valid || err)
+                break;
+            r = base.result;
+            r.iterations = ++total;
+            betaSecond = r.beta[second];
+            if (base.norm < O().fugacityTol)
+            {
+                r.converged = true;
+                r.presence = presenceFromFractions(r.beta);
+                deriveReferenceK(r);
+                updateSaturations(P, T, r);
+                return;
+            }
+            double J[NC][NC];
+            bool jacobianValid = true;
+#pragma unroll 1
+            for (int col = 0; col < NC; ++col)
+            {
+                double pert[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    pert[i] = logK[i];
+                const double step = O().fdStep * smax(1.0, fabs(logK[col]));
+                pert[col] += step;
+                evalTwo(P, T, z, first, second, pert, betaSecond, probe);
+                if (!probe.valid)
+                {
+                    jacobianValid = false;
+                    break;
+                }
+#pragma unroll
+                for (int row = 0; row < NC; ++row)
+                    J[row][col] = (probe.residual[row] - base.residual[row]) / step;
+            }
+            if (!jacobianValid)
+                break;
+            double rhs[NC], delta[NC];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                rhs[i] = -base.residual[i];
+            if (!solveDense<NC>(J, rhs, delta))
+                break;
+            bool accepted = false;
+            double damping = 1.0;
+#pragma unroll 1
+            for (int ls = 0; ls < 16; ++ls)
+            {
+                double trialLogK[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    trialLogK[i] = logK[i] + damping * delta[i];
+                evalTwo(P, T, z, first, second, trialLogK, betaSecond, probe);
+                if (probe.valid && probe.norm < base.norm)
+                {
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        logK[i] = trialLogK[i];
+                    accepted = true;
+                    break;
+                }
+                damping *= 0.5;
+            }
+            if (!accepted)
+                break;
+        }
+#pragma unroll 1
+        for (int it = ssiSteps; it < O().maxIterations; ++it)
+        {
+            if (err)
+                return;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                K[i] = exp(sclamp(logK[i], -230.0, 230.0));
+            if (!twoSsiStep(P, T, z, first, second, K, betaSecond, total, r))
+                return;
+            if (r.converged)
+                return;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                logK[i] = log(K[i]);
+        }
+    }
+
+    // finalizePhysicallyConvergedTwoPhase_ (restricted.inc:336-412)
+    __device__ void finalizePhysicallyConvergedTwoPhase(double P, double T, const double *z, int first,
+                                                        int second, Result<NC> &r)
+    {
+        if (r.converged)
+            return;
+        const double betaA = r.beta[first];
+        const double betaB = r.beta[second];
+        if (!(betaA > O().betaTol) || !(betaB > O().betaTol) || !isfinite(betaA) || !isfinite(betaB))
+            return;
+        const double betaClosure = fabs(betaA + betaB - 1.0);
+        const double closureTol = smax(O().fugacityTol, 10.0 * O().rrTol);
+        if (betaClosure > closureTol)
+            return;
+        double xa[NC], xb[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            xa[i] = r.x[first][i];
+            xb[i] = r.x[second][i];
+        }
+        normalize(xa);
+        normalize(xb);
+        double materialClosure = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double rec = betaA * xa[i] + betaB * xb[i];
+            materialClosure = smax(materialClosure, fabs(rec - z[i]));
+        }
+        if (materialClosure > closureTol)
+            return;
+        double phiA[NC], phiB[NC];
+        const double ZA = phase(first, P, T, xa, phiA);
+        const double ZB = phase(second, P, T, xb, phiB);
+        double fugacityResidual = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double aA = smax(xa[i] * phiA[i], 1.0e-300);
+            const double aB = smax(xb[i] * phiB[i], 1.0e-300);
+            fugacityResidual = smax(fugacityResidual, fabs(log(aA / aB)));
+        }
+        if (fugacityResidual > O().fugacityTol)
+            return;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            r.x[first][i] = xa[i];
+            r.x[second][i] = xb[i];
+        }
+        r.presence = uint8_t(bitOf(first) | bitOf(second));
+        r.Z[first] = ZA;
+        r.Z[second] = ZB;
+        r.converged = true;
+        deriveReferenceK(r);
+        updateSaturations(P, T, r);
+    }
+
+    // ------------------------------------------------------- three-phase ---
+    // evaluateThreePhaseLogK_ (nonlinear.inc:200-277)
+    __device__ __noinline__ void evalThree(double P, double T, const double *z, const double *logK,
+                                           double preferredGas, double preferredWater,
+                                           ThreePhaseLogKState<NC> &s)
+    {
+        s.valid = false;
+        s.norm = __longlong_as_double(0x7ff0000000000000LL);
+        s.result.init();
+        double kg[NC], kw[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            kg[i] = exp(sclamp(logK[i], -230.0, 230.0));
+            kw[i] = exp(sclamp(logK[NC + i], -230.0, 230.0));
+        }
+        double bg, bw;
+        if (!rr3Robust(z, kg, kw, preferredGas, preferredWater, bg, bw))
+            return;
+        const double bo = 1.0 - bg - bw;
+        if (!(bo >= -O().betaTol) || !(bg >= -O().betaTol) || !(bw >= -O().betaTol))
+            return;
+        double xo[NC], yg[NC], xw[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double D = bo + bg * kg[i] + bw * kw[i];
+            if (!(D > 0.0) || !isfinite(D))
+                return;
+            xo[i] = z[i] / D;
+            yg[i] = kg[i] * xo[i];
+            xw[i] = kw[i] * xo[i];
+        }
+        normalize(xo);
+        normalize(yg);
+        normalize(xw);
+        double phiO[NC], phiG[NC], phiW[NC];
+        const double Zo = phase(OIL, P, T, xo, phiO);
+        const double Zg = phase(GAS, P, T, yg, phiG);
+        const double Zw = phase(WATER, P, T, xw, phiW);
+        s.norm = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double po = smax(phiO[i], 1.0e-300);
+            const double pg = smax(phiG[i], 1.0e-300);
+            const double pw = smax(phiW[i], 1.0e-300);
+            s.residual[i] = logK[i] - log(po / pg);
+            s.residual[NC + i] = logK[NC + i] - log(po / pw);
+            s.norm = smax3(s.norm, fabs(s.residual[i]), fabs(s.residual[NC + i]));
+        }
+        Result<NC> &r = s.result;
+        r.presence = ALL_BITS;
+        r.beta[0] = bo; r.beta[1] = bg; r.beta[2] = bw;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            r.x[0][i] = xo[i];
+            r.x[1][i] = yg[i];
+            r.x[2][i] = xw[i];
+            r.Kg[i] = kg[i];
+            r.Kw[i] = kw[i];
+        }
+        r.Z[0] = Zo; r.Z[1] = Zg; r.Z[2] = Zw;
+        s.valid = isfinite(s.norm);
+    }
+
+    // one damped SSI step of flashThree_ (nonlinear.inc:301-371)
+    __device__ bool threeSsiStep(double P, double T, const double *z, double *kg, double *kw,
+                                 double &bg, double &bw, int &total, Result<NC> &r)
+    {
+        double ng, nw;
+        if (!rr3Robust(z, kg, kw, bg, bw, ng, nw))
+            return false;
+        bg = ng;
+        bw = nw;
+        const double bo = 1.0 - bg - bw;
+        double xo[NC], yg[NC], xw[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double D = bo + bg * kg[i] + bw * kw[i];
+            if (!(D > 0.0) || !isfinite(D))
+                return false;
+            xo[i] = z[i] / D;
+            yg[i] = kg[i] * xo[i];
+            xw[i] = kw[i] * xo[i];
+        }
+        normalize(xo);
+        normalize(yg);
+        normalize(xw);
+        double phiO[NC], phiG[NC], phiW[NC];
+        const double Zo = phase(OIL, P, T, xo, phiO);
+        const double Zg = phase(GAS, P, T, yg, phiG);
+        const double Zw = phase(WATER, P, T, xw, phiW);
+        double maxResidual = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double po = smax(phiO[i], 1.0e-300);
+            const double targetKg = po / smax(phiG[i], 1.0e-300);
+            const double targetKw = po / smax(phiW[i], 1.0e-300);
+            const double dg = sclamp(log(targetKg / kg[i]), -O().logKLimit, O().logKLimit);
+            const double dw = sclamp(log(targetKw / kw[i]), -O().logKLimit, O().logKLimit);
+            maxResidual = smax3(maxResidual, fabs(dg), fabs(dw));
+            kg[i] *= exp(0.6 * dg);
+            kw[i] *= exp(0.6 * dw);
+            kg[i] = sclamp(kg[i], 1.0e-100, 1.0e100);
+            kw[i] = sclamp(kw[i], 1.0e-100, 1.0e100);
+        }
+        ++total;
+        r.iterations = total;
+        r.beta[0] = bo; r.beta[1] = bg; r.beta[2] = bw;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            r.x[0][i] = xo[i];
+            r.x[1][i] = yg[i];
+            r.x[2][i] = xw[i];
+            r.Kg[i] = kg[i];
+            r.Kw[i] = kw[i];
+        }
+        r.Z[0] = Zo; r.Z[1] = Zg; r.Z[2] = Zw;
+        if (maxResidual < O().fugacityTol)
+        {
+            r.converged = true;
+            r.presence = presenceFromFractions(r.beta);
+            updateSaturations(P, T, r);
+        }
+        return true;
+    }
+
+    // flashThree_ (nonlinear.inc:279-513)
+    __device__ __noinline__ void flashThree(double P, double T, const double *z, const double *kgIn,
+                                            const double *kwIn, Result<NC> &r)
+    {
+        r.init();
+        r.presence = ALL_BITS;
+        double kg[NC], kw[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            kg[i] = sclamp(kgIn[i], 1.0e-100, 1.0e100);
+            kw[i] = sclamp(kwIn[i], 1.0e-100, 1.0e100);
+        }
+        double bg = 0.15, bw = 0.15;
+        const int ssiSteps = min(O().maxIterations, max(O().threeSsi, 0));
+        int total = 0;
+#pragma unroll 1
+        for (int it = 0; it < ssiSteps; ++it)
+        {
+            if (!threeSsiStep(P, T, z, kg, kw, bg, bw, total, r))
+                return;
+            if (r.converged || err)
+                return;
+        }
+        constexpr int M = 2 * NC;
+        double logK[M];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            logK[i] = log(kg[i]);
+            logK[NC + i] = log(kw[i]);
+        }
+        ThreePhaseLogKState<NC> base, probe;
+#pragma unroll 1
+        for (int it = 0; it < O().threeNewton; ++it)
+        {
+            evalThree(P, T, z, logK, bg, bw, base);
+            if (!base.valid || err)
+                break;
+            r = base.result;
+            r.iterations = ++total;
+            bg = r.beta[1];
+            bw = r.beta[2];
+            if (base.norm < O().fugacityTol)
+            {
+                r.converged = true;
+                r.presence = presenceFromFractions(r.beta);
+                updateSaturations(P, T, r);
+                return;
+            }
+            double J[M][M];
+            bool jacobianValid = true;
+#pragma unroll 1
+            for (int col = 0; col < M; ++col)
+            {
+                const double step = O().fdStep * smax(1.0, fabs(logK[col]));
+                double pert[M];
+#pragma unroll
+                for (int i = 0; i < M; ++i)
+                    pert[i] = logK[i];
+                pert[col] += step;
+                evalThree(P, T, z, pert, bg, bw, probe);
+                if (probe.valid)
+                {
+#pragma unroll
+                    for (int row = 0; row < M; ++row)
+                        J[row][col] = (probe.residual[row] - base.residual[row]) / step;
+                    continue;
+                }
+#pragma unroll
+                for (int i = 0; i < M; ++i)
+                    pert[i] = logK[i];
+                pert[col] -= step;
+                evalThree(P, T, z, pert, bg, bw, probe);
+                if (!probe.valid)
+                {
+                    jacobianValid = false;
+                    break;
+                }
+#pragma unroll
+                for (int row = 0; row < M; ++row)
+                    J[row][col] = (base.residual[row] - probe.residual[row]) / step;
+            }
+            if (!jacobianValid)
+                break;
+            double rhs[M], delta[M];
+#pragma unroll
+            for (int i = 0; i < M; ++i)
+                rhs[i] = -base.residual[i];
+            if (!solveDense<M>(J, rhs, delta))
+                break;
+            bool accepted = false;
+            double damping = 1.0;
+#pragma unroll 1
+            for (int ls = 0; ls < 16; ++ls)
+            {
+                double trialLogK[M];
+#pragma unroll
+                for (int i = 0; i < M; ++i)
+                    trialLogK[i] = logK[i] + damping * delta[i];
+                evalThree(P, T, z, trialLogK, bg, bw, probe);
+                if (probe.valid && probe.norm < base.norm)
+                {
+#pragma unroll
+                    for (int i = 0; i < M; ++i)
+                        logK[i] = trialLogK[i];
+                    accepted = true;
+                    break;
+                }
+                damping *= 0.5;
+            }
+            if (!accepted)
+                break;
+        }
+#pragma unroll 1
+        for (int it = ssiSteps; it < O().maxIterations; ++it)
+        {
+            if (err)
+                return;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+            {
+                kg[i] = exp(sclamp(logK[i], -230.0, 230.0));
+                kw[i] = exp(sclamp(logK[NC + i], -230.0, 230.0));
+            }
+            if (!threeSsiStep(P, T, z, kg, kw, bg, bw, total, r))
+                return;
+            if (r.converged)
+                return;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+            {
+                logK[i] = log(kg[i]);
+                logK[NC + i] = log(kw[i]);
+            }
+        }
+    }
+
+    // ----------------------------------------------------- stability -------
+    // evaluateStabilityResidual_ (stability.inc:157-204)
+    __device__ void stabilityResidual(int candidate, double P, double T, const double *logRef,
+                                      const double *logW, StabilityResidual<NC> &s)
+    {
+        s.valid = false;
+        double maxLogW = logW[0];
+#pragma unroll
+        for (int i = 1; i < NC; ++i)
+            if (maxLogW < logW[i])
+                maxLogW = logW[i];
+        if (!isfinite(maxLogW))
+            return;
+        double scaledSum = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double v = exp(logW[i] - maxLogW);
+            if (!(v > 0.0) || !isfinite(v))
+                return;
+            s.x[i] = v;
+            scaledSum += v;
+        }
+        if (!(scaledSum > 0.0) || !isfinite(scaledSum))
+            return;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            s.x[i] /= scaledSum;
+        const double logSum = maxLogW + log(scaledSum);
+        s.sum = logSum > 709.782712893384 ? __longlong_as_double(0x7ff0000000000000LL) : exp(logSum);
+        phase(candidate, P, T, s.x, s.phi);
+        s.norm = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double phi = s.phi[i];
+            if (!(phi > 0.0) || !isfinite(phi))
+                return;
+            s.residual[i] = logW[i] + log(phi) - logRef[i];
+            s.norm = smax(s.norm, fabs(s.residual[i]));
+        }
+        s.valid = isfinite(s.norm);
+    }
+
+    // finalizeStabilityTrial_ (stability.inc:206-223)
+    __device__ void finalizeTrial(const StabilityResidual<NC> &s, const double *ref, Trial<NC> &t) const
+    {
+        double dist = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            dist += fabs(s.x[i] - ref[i]);
+        t.valid = true;
+        t.trivial = dist < 1.0e-7 && fabs(s.sum - 1.0) < 1.0e-7;
+        t.sum = s.sum;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            t.x[i] = s.x[i];
+    }
+
+    // stabilityTrial_ (stability.inc:225-355)
+    __device__ __noinline__ void stabilityTrial(int candidate, double P, double T, const double *logRef,
+                                                const double *ref, const double *seedIn, Trial<NC> &t)
+    {
+        t.valid = false;
+        t.trivial = false;
+        t.sum = 0.0;
+        double seed[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            seed[i] = seedIn[i];
+        normalize(seed);
+        double logW[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            logW[i] = log(smax(seed[i], O().floor));
+        const int ssiSteps = min(O().maxStability, max(O().stabilitySsi, 0));
+        StabilityResidual<NC> cur, probe;
+#pragma unroll 1
+        for (int it = 0; it < ssiSteps; ++it)
+        {
+            stabilityResidual(candidate, P, T, logRef, logW, cur);
+            if (!cur.valid || err)
+                return;
+            if (cur.norm < O().stabilityTol)
+            {
+                finalizeTrial(cur, ref, t);
+                return;
+            }
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                logW[i] = logRef[i] - log(smax(cur.phi[i], 1.0e-300));
+        }
+#pragma unroll 1
+        for (int it = 0; it < O().stabilityNewton; ++it)
+        {
+            stabilityResidual(candidate, P, T, logRef, logW, cur);
+            if (!cur.valid || err)
+                return;
+            if (cur.norm < O().stabilityTol)
+            {
+                finalizeTrial(cur, ref, t);
+                return;
+            }
+            double J[NC][NC];
+#pragma unroll 1
+            for (int col = 0; col < NC; ++col)
+            {
+                double pert[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    pert[i] = logW[i];
+                const double step = O().fdStep * smax(1.0, fabs(logW[col]));
+                pert[col] += step;
+                stabilityResidual(candidate, P, T, logRef, pert, probe);
+                if (!probe.valid)
+                    return;
+#pragma unroll
+                for (int row = 0; row < NC; ++row)
+                    J[row][col] = (probe.residual[row] - cur.residual[row]) / step;
+            }
+            double rhs[NC], delta[NC];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                rhs[i] = -cur.residual[i];
+            if (!solveDense<NC>(J, rhs, delta))
+                break;
+            bool accepted = false;
+            double damping = 1.0;
+#pragma unroll 1
+            for (int ls = 0; ls < 16; ++ls)
+            {
+                double cand[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    cand[i] = logW[i] + damping * delta[i];
+                stabilityResidual(candidate, P, T, logRef, cand, probe);
+                if (probe.valid && probe.norm < cur.norm)
+                {
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        logW[i] = cand[i];
+                    accepted = true;
+                    break;
+                }
+                damping *= 0.5;
+            }
+            if (!accepted)
+                break;
+        }
+        const int remaining = max(0, O().maxStability - ssiSteps);
+#pragma unroll 1
+        for (int it = 0; it < remaining; ++it)
+        {
+            stabilityResidual(candidate, P, T, logRef, logW, cur);
+            if (!cur.valid || err)
+                return;
+            if (cur.norm < O().stabilityTol)
+            {
+                finalizeTrial(cur, ref, t);
+                return;
+            }
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                logW[i] = logRef[i] - log(smax(cur.phi[i], 1.0e-300));
+        }
+    }
+
+    // stabilitySeeds_ (stability.inc:32-96): seed k of the candidate list.
+    __device__ int stabilitySeedCount() const { return NC + 6 + ((F->water >= 0 && NC > 1) ? 1 : 0); }
+
+    __device__ void stabilitySeed(int k, double P, double T, const double *z, const double *ref, double *seed)
+    {
+        if (k < 4)
+        {
+            const double exps[4] = {1.0, -1.0, 1.0 / 3.0, -1.0 / 3.0};
+            double wilson[NC];
+            wilsonK(P, T, wilson);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+            {
+                const double kk = sclamp(wilson[i], 1.0e-100, 1.0e100);
+                seed[i] = z[i] * pow(kk, exps[k]);
+            }
+            normalize(seed);
+            return;
+        }
+        k -= 4;
+        if (k < NC)
+        {
+            const double remainder = 0.1 / double(NC - 1);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                seed[i] = remainder;
+            seed[k] = 0.9;
+            return;
+        }
+        k -= NC;
+        if (k == 0 || k == 1)
+        {
+            const double *src = k == 0 ? z : ref;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                seed[i] = src[i];
+            normalize(seed);
+            return;
+        }
+        const double trace = 1.0e-6 / double(NC - 1);
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            seed[i] = trace;
+        seed[F->water] = 1.0 - 1.0e-6;
+    }
+
+    // stabilityTest (three_phase_flash.hpp:300-489)
+    __device__ __noinline__ void stabilityTest(double P, double T, const double *zIn, uint8_t active,
+                                               const double (&activeX)[3][NC], StabilityResult<NC> &res)
+    {
+        res.stable = true;
+        res.valid = true;
+        res.tested = active;
+        for (int p = 0; p < 3; ++p)
+        {
+            res.unstable[p] = false;
+            res.trialSum[p] = 1.0;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                res.incipient[p][i] = 0.0;
+        }
+        if (!validatePT(P, T))
+            return;
+        if (active == 0)
+        {
+            fail(ERR_BAD_INPUT);
+            return;
+        }
+        double z[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            z[i] = zIn[i];
+        normalize(z);
+        const int ref = firstActive(active);
+        double sx[3][NC];
+        for (int p = 0; p < 3; ++p)
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                sx[p][i] = activeX[p][i];
+        if (sw() && popcount3(active) == 1)
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                sx[ref][i] = z[i];
+        for (int p = 0; p < 3; ++p)
+            if (active & bitOf(p))
+                normalize(sx[p]);
+
+        if (sw() && popcount3(active) > 1)
+        {
+            // fugacity-closure certification of the supplied active set (:310-367)
+            double phiR[NC], phiP[NC];
+            phase(ref, P, T, sx[ref], phiR);
+            double mismatch = 0.0;
+            for (int p = 0; p < 3; ++p)
+            {
+                if (!(active & bitOf(p)) || p == ref)
+                    continue;
+                phase(p, P, T, sx[p], phiP);
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                {
+                    const double xr = sx[ref][i];
+                    const double xp = sx[p][i];
+                    if (xr <= 10.0 * O().floor || xp <= 10.0 * O().floor)
+                        continue;
+                    const double ra = smax(xr * phiR[i], 1.0e-300);
+                    const double pa = smax(xp * phiP[i], 1.0e-300);
+                    mismatch = smax(mismatch, fabs(log(ra / pa)));
+                }
+            }
+            const double certTol = smax(10.0 * O().fugacityTol, 10.0 * O().stabilityTol);
+            if (mismatch > certTol)
+            {
+                Result<NC> certified;
+                flashRestrictedImpl(P, T, z, active, &sx, certified);
+                if (!certified.converged || certified.presence != active)
+                {
+                    res.valid = false;
+                    res.stable = false;
+                    return;
+                }
+                for (int p = 0; p < 3; ++p)
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        sx[p][i] = certified.x[p][i];
+            }
+        }
+
+        double refX[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            refX[i] = sx[ref][i];
+        normalize(refX);
+        double phiRef[NC];
+        phase(ref, P, T, refX, phiRef);
+        double logRef[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double xi = smax(refX[i], O().floor);
+            const double ph = smax(phiRef[i], 1.0e-300);
+            logRef[i] = log(xi) + log(ph);
+        }
+        const double coincTol = smax(10.0 * O().coincidentTol, 1.0e-7);
+        for (int cand = 0; cand < 3; ++cand)
+        {
+            if (active & bitOf(cand))
+                continue;
+            Trial<NC> best, trial;
+            best.valid = false;
+            best.trivial = false;
+            best.sum = -__longlong_as_double(0x7ff0000000000000LL);
+            const int nseeds = stabilitySeedCount();
+#pragma unroll 1
+            for (int k = 0; k < nseeds; ++k)
+            {
+                double seed[NC];
+                stabilitySeed(k, P, T, z, refX, seed);
+                stabilityTrial(cand, P, T, logRef, refX, seed, trial);
+                if (trial.valid && (!best.valid || trial.sum > best.sum))
+                    best = trial;
+                if (err)
+                    return;
+            }
+            if (!best.valid)
+            {
+                res.valid = false;
+                res.stable = false;
+                continue;
+            }
+            res.trialSum[cand] = best.sum;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                res.incipient[cand][i] = best.x[i];
+            bool coincides = false;
+            for (int p = 0; p < 3; ++p)
+            {
+                if (!(active & bitOf(p)))
+                    continue;
+                double maxDiff = 0.0;
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    maxDiff = smax(maxDiff, fabs(best.x[i] - sx[p][i]));
+                if (maxDiff <= coincTol)
+                {
+                    coincides = true;
+                    break;
+                }
+            }
+            const bool unstable = !best.trivial && !coincides && best.sum > 1.0 + O().stabilityTol;
+            res.unstable[cand] = unstable;
+            res.stable = res.stable && !unstable;
+        }
+    }
+
+    // --------------------------------------------------- canonicalisation --
+    // refreshCanonicalThermodynamics_ (canonicalization.inc:47-66)
+    __device__ void refreshCanonical(double P, double T, Result<NC> &r)
+    {
+        double phi[NC];
+        for (int p = 0; p < 3; ++p)
+        {
+            if (!(r.presence & bitOf(p)))
+                continue;
+            normalize(r.x[p]);
+            r.Z[p] = phase(p, P, T, r.x[p], phi);
+        }
+        deriveReferenceK(r);
+        updateSaturations(P, T, r);
+    }
+
+    // canonicalizeLiquidRoles_ (canonicalization.inc:99-135)
+    __device__ void canonicalizeLiquidRoles(Result<NC> &r) const
+    {
+        if (F->water < 0)
+            return;
+        const bool hasOil = r.beta[0] > O().betaTol;
+        const bool hasWater = r.beta[2] > O().betaTol;
+        bool swap = false;
+        if (hasOil && hasWater)
+        {
+            swap = r.x[0][F->water] > r.x[2][F->water];
+        }
+        else if (hasOil != hasWater)
+        {
+            const int act = hasOil ? 0 : 2;
+            const bool shouldBeWater = waterIsDominant(r.x[act]);
+            swap = (hasOil && shouldBeWater) || (hasWater && !shouldBeWater);
+        }
+        if (swap)
+            swapSlots(r, 0, 2);
+    }
+
+    // canonicalize_ (canonicalization.inc:8-45)
+    __device__ __noinline__ void canonicalize(double P, double T, Result<NC> &r)
+    {
+        uint8_t p = presenceFromFractions(r.beta);
+        if (p == 0)
+            p = r.presence == 0 ? OIL_BIT : r.presence;
+        r.presence = p;
+        double sum = 0.0;
+        for (int i = 0; i < 3; ++i)
+        {
+            double &beta = r.beta[i];
+            if (!(p & bitOf(i)) || beta <= O().betaTol || !isfinite(beta))
+            {
+                beta = 0.0;
+                r.presence &= uint8_t(~bitOf(i));
+            }
+            else
+            {
+                sum += beta;
+            }
+        }
+        if (!(sum > 0.0))
+        {
+            r.presence = chooseSinglePhase(P, T, r.x[0]);
+            r.beta[0] = r.beta[1] = r.beta[2] = 0.0;
+            r.beta[firstActive(r.presence)] = 1.0;
+        }
+        else
+        {
+            for (int i = 0; i < 3; ++i)
+                r.beta[i] /= sum;
+        }
+        if (!sw())
+            canonicalizeLiquidRoles(r);
+        r.presence = presenceFromFractions(r.beta);
+        refreshCanonical(P, T, r);
+    }
+
+    // canonicalizeGlobalWaterRole_ (canonicalization.inc:175-224)
+    __device__ int canonicalizeGlobalWaterRole(Result<NC> &r) const
+    {
+        if (F->water < 0)
+            return -1;
+        const int wc = F->water;
+        int richest = 2;
+        double richestWater = -1.0;
+        int activeCount = 0;
+        bool hasWaterSlot = false;
+        for (int s = 0; s < 3; ++s)
+        {
+            if (!(r.beta[s] > O().betaTol))
+                continue;
+            ++activeCount;
+            if (s == 2)
+                hasWaterSlot = true;
+            const double xw = r.x[s][wc];
+            if (xw > richestWater)
+            {
+                richestWater = xw;
+                richest = s;
+            }
+        }
+        if (activeCount == 0 || richest == 2)
+            return -1;
+        if (!hasWaterSlot && !waterIsDominant(r.x[richest]))
+            return -1;
+        const double currentWater = hasWaterSlot ? r.x[2][wc] : -1.0;
+        if (hasWaterSlot && richestWater <= currentWater + 1.0e-10 * smax(1.0, fabs(richestWater)))
+            return -1;
+        swapSlots(r, richest, 2);
+        return richest;
+    }
+
+    // validatePhysicalFlashResult_ (canonicalization.inc:225-321)
+    __device__ __noinline__ bool validatePhysical(double P, double T, const double *z, const Result<NC> &r)
+    {
+        if (!r.converged)
+            return false;
+        const double tol = smax3(10.0 * O().fugacityTol, 10.0 * O().rrTol, 1.0e-10);
+        double betaSum = 0.0;
+        uint8_t active = 0;
+        for (int p = 0; p < 3; ++p)
+        {
+            const double beta = r.beta[p];
+            if (!isfinite(beta) || beta < -tol)
+                return false;
+            if (beta > O().betaTol)
+            {
+                active |= uint8_t(bitOf(p));
+                betaSum += beta;
+                double xsum = 0.0;
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                {
+                    const double xv = r.x[p][i];
+                    if (!isfinite(xv) || xv < -tol)
+                        return false;
+                    xsum += xv;
+                }
+                if (fabs(xsum - 1.0) > tol)
+                    return false;
+            }
+        }
+        if (active == 0 || fabs(betaSum - 1.0) > tol)
+            return false;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            double rec = 0.0;
+            for (int p = 0; p < 3; ++p)
+                if (active & bitOf(p))
+                    rec += r.beta[p] * r.x[p][i];
+            if (fabs(rec - z[i]) > tol)
+                return false;
+        }
+        if (popcount3(active) <= 1)
+            return true;
+        const int ref = firstActive(active);
+        double phiR[NC], phiP[NC];
+        phaseForRole(ref, P, T, r.x[ref], phiR);
+        for (int p = 0; p < 3; ++p)
+        {
+            if (!(active & bitOf(p)) || p == ref)
+                continue;
+            phaseForRole(p, P, T, r.x[p], phiP);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+            {
+                if (r.x[ref][i] <= 10.0 * O().floor || r.x[p][i] <= 10.0 * O().floor)
+                    continue;
+                const double ra = smax(r.x[ref][i] * phiR[i], 1.0e-300);
+                const double pa = smax(r.x[p][i] * phiP[i], 1.0e-300);
+                if (fabs(log(ra / pa)) > 10.0 * O().fugacityTol)
+                    return false;
+            }
+        }
+        return true;
+    }
+
+    // overallComposition_ (canonicalization.inc:323-337)
+    __device__ void overallComposition(const Result<NC> &r, double *z)
+    {
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            z[i] = 0.0;
+        for (int s = 0; s < 3; ++s)
+        {
+            const double beta = r.beta[s];
+            if (!(beta > O().betaTol))
+                continue;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                z[i] += beta * r.x[s][i];
+        }
+        normalize(z);
+    }
+
+    // reequilibrateCanonicalRoles_ (canonicalization.inc:339-377)
+    __device__ void reequilibrateCanonicalRoles(double P, double T, const double *z, Result<NC> &seed,
+                                                Result<NC> &out)
+    {
+        seed.presence = presenceFromFractions(seed.beta);
+        const int count = popcount3(seed.presence);
+        if (count <= 1)
+        {
+            singlePhaseResult(P, T, z, seed.presence, out);
+            return;
+        }
+        if (count == 2)
+        {
+            int first, second;
+            activePair(seed.presence, first, second);
+            double K[NC];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                K[i] = sclamp(seed.x[second][i] / smax(seed.x[first][i], O().floor), 1.0e-100, 1.0e100);
+            flashTwo(P, T, z, first, second, K, out);
+            return;
+        }
+        deriveReferenceK(seed);
+        flashThree(P, T, z, seed.Kg, seed.Kw, out);
+        if (out.converged)
+            return;
+        double kg[NC], kw[NC];
+        wilsonK(P, T, kg);
+        initialWaterK(kw);
+        flashThree(P, T, z, kg, kw, out);
+    }
+
+    // canonicalizeNonAqueousRoles_ (canonicalization.inc:379-414)
+    __device__ bool canonicalizeNonAqueousRoles(double P, double T, Result<NC> &r) const
+    {
+        const bool hasOil = r.beta[0] > O().betaTol;
+        const bool hasGas = r.beta[1] > O().betaTol;
+        if (!(hasOil && hasGas))
+            return false;
+        double wilson[NC];
+        wilsonK(P, T, wilson);
+        double orientation = 0.0, magnitude = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double lnK = log(sclamp(wilson[i], 1.0e-30, 1.0e30));
+            const double term = (r.x[1][i] - r.x[0][i]) * lnK;
+            orientation += term;
+            magnitude += fabs(term);
+        }
+        if (orientation >= -1.0e-10 * smax(1.0, magnitude))
+            return false;
+        swapSlots(r, 0, 1);
+        return true;
+    }
+
+    // expectedSingleNonAqueousRole_ (canonicalization.inc:416-439)
+    __device__ int expectedSingleNonAqueousRole(double P, double T, const double *x) const
+    {
+        double wilson[NC];
+        wilsonK(P, T, wilson);
+        double volatility = 0.0, magnitude = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double term = x[i] * log(sclamp(wilson[i], 1.0e-30, 1.0e30));
+            volatility += term;
+            magnitude += fabs(term);
+        }
+        return volatility >= -1.0e-10 * smax(1.0, magnitude) ? GAS : OIL;
+    }
+
+    // canonicalizeSingleNonAqueousRole_ (canonicalization.inc:441-463)
+    __device__ bool canonicalizeSingleNonAqueousRole(double P, double T, Result<NC> &r) const
+    {
+        const bool hasOil = r.beta[0] > O().betaTol;
+        const bool hasGas = r.beta[1] > O().betaTol;
+        if (hasOil == hasGas)
+            return false;
+        const int act = hasOil ? 0 : 1;
+        const int expected = expectedSingleNonAqueousRole(P, T, r.x[act]);
+        if (act == expected)
+            return false;
+        swapSlots(r, act, expected);
+        r.presence = presenceFromFractions(r.beta);
+        return true;
+    }
+
+    // canonicalizeCoalescedSwSingleNonAqueousRole_ (canonicalization.inc:466-498)
+    __device__ void canonicalizeCoalescedSwSingle(double P, double T, Result<NC> &r)
+    {
+        if (!sw())
+            return;
+        const bool hasOil = r.beta[0] > O().betaTol;
+        const bool hasGas = r.beta[1] > O().betaTol;
+        if (hasOil == hasGas)
+            return;
+        const int act = hasOil ? 0 : 1;
+        double phi[NC];
+        const double zo = phaseForRole(OIL, P, T, r.x[act], phi);
+        const double zg = phaseForRole(GAS, P, T, r.x[act], phi);
+        const double scale = smax3(1.0, fabs(zo), fabs(zg));
+        if (fabs(zo - zg) > 1.0e-8 * scale)
+            return;
+        (void)canonicalizeSingleNonAqueousRole(P, T, r);
+    }
+
+    // collapseCoincidentSwPhases_ (canonicalization.inc:507-586)
+    __device__ void collapseCoincidentSw(double P, double T, Result<NC> &r)
+    {
+        if (!sw() || !(O().coincidentTol > 0.0))
+            return;
+        const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+        bool changed = false;
+        for (int pass = 0; pass < 2; ++pass)
+        {
+            bool merged = false;
+            for (int k = 0; k < 3; ++k)
+            {
+                const int a = pairs[k][0], b = pairs[k][1];
+                const double betaA = r.beta[a], betaB = r.beta[b];
+                if (!(betaA > O().betaTol) || !(betaB > O().betaTol))
+                    continue;
+                double maxDiff = 0.0;
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    maxDiff = smax(maxDiff, fabs(r.x[a][i] - r.x[b][i]));
+                if (maxDiff > O().coincidentTol)
+                    continue;
+                const double combinedBeta = betaA + betaB;
+                double combined[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    combined[i] = (betaA * r.x[a][i] + betaB * r.x[b][i]) / combinedBeta;
+                int dest = a;
+                if (a == 2 || b == 2)
+                    dest = 2;
+                else
+                    dest = expectedSingleNonAqueousRole(P, T, combined);
+                const int src = dest == a ? b : a;
+                r.beta[dest] = combinedBeta;
+                r.beta[src] = 0.0;
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                {
+                    r.x[dest][i] = combined[i];
+                    r.x[src][i] = combined[i];
+                }
+                r.sat[src] = 0.0;
+                r.rho[src] = 0.0;
+                r.Z[src] = 1.0;
+                merged = true;
+                changed = true;
+                break;
+            }
+            if (!merged)
+                break;
+        }
+        if (!changed)
+            return;
+        r.presence = presenceFromFractions(r.beta);
+        refreshCanonical(P, T, r);
+    }
+
+    // swThermodynamicRolesConsistent_ (canonicalization.inc:588-686)
+    __device__ bool swRolesConsistent(double P, double T, const Result<NC> &r, bool preserveRestricted)
+    {
+        if (!sw() || F->water < 0)
+            return true;
+        const int wc = F->water;
+        int activeCount = 0, aqueousSlot = -1, oilSlot = -1, gasSlot = -1, richestSlot = -1;
+        double richestWater = -1.0;
+        for (int s = 0; s < 3; ++s)
+        {
+            if (!(r.beta[s] > O().betaTol))
+                continue;
+            ++activeCount;
+            const int role = roles[s];
+            if (role == WATER) aqueousSlot = s;
+            if (role == OIL) oilSlot = s;
+            if (role == GAS) gasSlot = s;
+            const double xw = r.x[s][wc];
+            if (xw > richestWater)
+            {
+                richestWater = xw;
+                richestSlot = s;
+            }
+        }
+        if (activeCount == 0)
+            return false;
+        if (aqueousSlot >= 0)
+        {
+            if (richestSlot != aqueousSlot &&
+                richestWater > r.x[aqueousSlot][wc] + 1.0e-10 * smax(1.0, fabs(richestWater)))
+                return false;
+        }
+        else if (richestSlot >= 0 && waterIsDominant(r.x[richestSlot]))
+        {
+            return false;
+        }
+        if ((oilSlot >= 0) != (gasSlot >= 0))
+        {
+            const int slot = oilSlot >= 0 ? oilSlot : gasSlot;
+            const double *x = r.x[slot];
+            bool coalesced = false;
+            if (preserveRestricted)
+            {
+                double phi[NC];
+                const double zo = phaseForRole(OIL, P, T, x, phi);
+                const double zg = phaseForRole(GAS, P, T, x, phi);
+                const double scale = smax3(1.0, fabs(zo), fabs(zg));
+                coalesced = fabs(zo - zg) <= 1.0e-8 * scale;
+            }
+            if (!coalesced)
+            {
+                double pseudoTc = 0.0;
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    pseudoTc += x[i] * F->tc[i];
+                const double scale = smax3(1.0, fabs(T), fabs(pseudoTc));
+                if (fabs(T - pseudoTc) > 1.0e-8 * scale)
+                {
+                    const int expected = T > pseudoTc ? GAS : OIL;
+                    if (roles[slot] != expected)
+                        return false;
+                }
+            }
+        }
+        return true;
+    }
+
+    // canonicalizeSwThermodynamicRoles_ (canonicalization.inc:688-712)
+    __device__ void canonicalizeSwRoles(Result<NC> &r) const
+    {
+        Result<NC> c = r;
+        for (int p = 0; p < 3; ++p)
+        {
+            c.beta[p] = 0.0;
+            c.sat[p] = 0.0;
+            c.Z[p] = 1.0;
+            c.rho[p] = 0.0;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                c.x[p][i] = 0.0;
+        }
+        for (int s = 0; s < 3; ++s)
+        {
+            const int phys = roles[s];
+            c.beta[phys] = r.beta[s];
+            c.sat[phys] = r.sat[s];
+            c.Z[phys] = r.Z[s];
+            c.rho[phys] = r.rho[s];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                c.x[phys][i] = r.x[s][i];
+        }
+        c.presence = presenceFromFractions(c.beta);
+        deriveReferenceK(c);
+        r = c;
+    }
+
+    // canonicalizeFinal_ (canonicalization.inc:714-796)
+    __device__ __noinline__ void canonicalizeFinal(double P, double T, Result<NC> &r, bool preserveRestricted)
+    {
+        if (!r.converged)
+            return;
+        if (sw())
+        {
+            if (!swRolesConsistent(P, T, r, preserveRestricted))
+            {
+                r.converged = false;
+                return;
+            }
+            canonicalizeSwRoles(r);
+            collapseCoincidentSw(P, T, r);
+            if (!preserveRestricted)
+                canonicalizeCoalescedSwSingle(P, T, r);
+            (void)canonicalizeNonAqueousRoles(P, T, r);
+            r.presence = presenceFromFractions(r.beta);
+            return;
+        }
+        for (int pass = 0; pass < 4; ++pass)
+        {
+            r.presence = presenceFromFractions(r.beta);
+            double z[NC];
+            overallComposition(r, z);
+            const int waterSource = canonicalizeGlobalWaterRole(r);
+            const bool crossedGasWater = waterSource == GAS;
+            const bool crossedSingle = !preserveRestricted && canonicalizeSingleNonAqueousRole(P, T, r);
+            if (crossedGasWater || crossedSingle)
+            {
+                r.presence = presenceFromFractions(r.beta);
+                Result<NC> corrected;
+                reequilibrateCanonicalRoles(P, T, z, r, corrected);
+                if (!corrected.converged)
+                {
+                    r.converged = false;
+                    return;
+                }
+                r = corrected;
+                continue;
+            }
+            (void)canonicalizeNonAqueousRoles(P, T, r);
+            r.presence = presenceFromFractions(r.beta);
+            refreshCanonical(P, T, r);
+            return;
+        }
+        r.converged = false;
+    }
+
+    // ------------------------------------------------------- active set ----
+    // equilibrateActiveSet_ (allocation.inc:707-858)
+    __device__ __noinline__ void equilibrateActiveSet(double P, double T, const double *z, uint8_t active,
+                                                      Result<NC> &seed, bool reuseConvergedSeed,
+                                                      Result<NC> &out)
+    {
+        if (active == 0)
+            active = chooseSinglePhase(P, T, z);
+        canonicalize(P, T, seed);
+        if (seed.presence != active)
+            active = seed.presence;
+        Result<NC> lastPhysical = seed;
+        bool useConvergedSeed = reuseConvergedSeed && seed.converged && seed.presence == active && !sw();
+        Result<NC> &current = out;
+#pragma unroll 1
+        for (int outer = 0; outer < 8; ++outer)
+        {
+            if (err)
+            {
+                out.converged = false;
+                return;
+            }
+            if (useConvergedSeed)
+            {
+                current = seed;
+                useConvergedSeed = false;
+            }
+            else if (popcount3(active) == 1)
+            {
+                singlePhaseResult(P, T, z, active, current);
+            }
+            else if (popcount3(active) == 2)
+            {
+                int first, second;
+                activePair(active, first, second);
+                double K[NC];
+                pairInitialK(first, second, P, T, z, K);
+                if (seed.converged && seed.presence == active)
+                {
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        K[i] = sclamp(seed.x[second][i] / smax(seed.x[first][i], O().floor),
+                                      1.0e-100, 1.0e100);
+                }
+                flashTwo(P, T, z, first, second, K, current);
+                if (!current.converged)
+                    singlePhaseResult(P, T, z, chooseSinglePhase(P, T, z), current);
+            }
+            else
+            {
+                double kg[NC], kw[NC];
+                bool kgValid = true, kwValid = true;
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                {
+                    kg[i] = seed.Kg[i];
+                    kw[i] = seed.Kw[i];
+                    kgValid = kgValid && kg[i] > 0.0;
+                    kwValid = kwValid && kw[i] > 0.0;
+                }
+                if (!kgValid) wilsonK(P, T, kg);
+                if (!kwValid) initialWaterK(kw);
+                flashThree(P, T, z, kg, kw, current);
+                if (!current.converged)
+                {
+                    lastPhysical.converged = false;
+                    canonicalize(P, T, lastPhysical);
+                    out = lastPhysical;
+                    return;
+                }
+            }
+
+            uint8_t fractionPresence = presenceFromFractions(current.beta);
+            if (fractionPresence == 0)
+                fractionPresence = chooseSinglePhase(P, T, z);
+            if (fractionPresence != active)
+            {
+                active = fractionPresence;
+                seed = current;
+                canonicalize(P, T, seed);
+                lastPhysical = seed;
+                useConvergedSeed = seed.converged && seed.presence == active && !sw();
+                continue;
+            }
+            canonicalize(P, T, current);
+            lastPhysical = current;
+            if (popcount3(active) == 3)
+            {
+                canonicalize(P, T, current);
+                return;
+            }
+            StabilityResult<NC> st;
+            stabilityTest(P, T, z, active, current.x, st);
+            if (!st.valid)
+            {
+                current.converged = false;
+                canonicalize(P, T, current);
+                return;
+            }
+            if (st.stable)
+            {
+                canonicalize(P, T, current);
+                return;
+            }
+            bool added = false;
+            for (int p = 0; p < 3; ++p)
+            {
+                if (!(active & bitOf(p)) && st.unstable[p])
+                {
+                    active |= uint8_t(bitOf(p));
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        seed.x[p][i] = st.incipient[p][i];
+                    added = true;
+                }
+            }
+            if (!added)
+            {
+                current.converged = false;
+                canonicalize(P, T, current);
+                return;
+            }
+            deriveReferenceK(seed);
+            seed.presence = active;
+            useConvergedSeed = false;
+        }
+        canonicalize(P, T, seed);
+        out = seed;
+    }
+
+    // ------------------------------------------------- restricted flashes --
+    // flashRestrictedImpl_ (restricted.inc:8-59).  A three-phase `allowed`
+    // set is never requested by the entry points carried here.
+    __device__ __noinline__ void flashRestrictedImpl(double P, double T, const double *zIn, uint8_t allowed,
+                                                     const double (*seedX)[3][NC], Result<NC> &r)
+    {
+        r.init();
+        if (!validatePT(P, T))
+            return;
+        double z[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            z[i] = zIn[i];
+        normalize(z);
+        if (allowed == 0)
+        {
+            fail(ERR_BAD_INPUT);
+            return;
+        }
+        if (popcount3(allowed) == 3)
+        {
+            fail(ERR_NOT_PORTED);
+            return;
+        }
+        if (popcount3(allowed) == 1)
+        {
+            singlePhaseResult(P, T, z, allowed, r);
+            return;
+        }
+        int first, second;
+        activePair(allowed, first, second);
+        double K[NC];
+        pairInitialK(first, second, P, T, z, K);
+        if (seedX != nullptr)
+        {
+            double a[NC], b[NC];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+            {
+                a[i] = (*seedX)[first][i];
+                b[i] = (*seedX)[second][i];
+            }
+            normalize(a);
+            normalize(b);
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                K[i] = sclamp(b[i] / smax(a[i], O().floor), 1.0e-100, 1.0e100);
+        }
+        flashTwo(P, T, z, first, second, K, r);
+        if (!r.converged && seedX != nullptr)
+        {
+            pairInitialK(first, second, P, T, z, K);
+            flashTwo(P, T, z, first, second, K, r);
+        }
+        if (r.converged)
+            canonicalize(P, T, r);
+    }
+
+    // flashRestricted (three_phase_flash.hpp:235-292), both overloads
+    __device__ __noinline__ void flashRestricted(double P, double T, const double *zIn, uint8_t allowed,
+                                                 const double (*seedX)[3][NC], Result<NC> &r)
+    {
+        double z[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            z[i] = zIn[i];
+        normalize(z);
+        flashRestrictedImpl(P, T, z, allowed, seedX, r);
+        if (!r.converged && popcount3(allowed) == 2 && sw())
+        {
+            int first, second;
+            activePair(allowed, first, second);
+            finalizePhysicallyConvergedTwoPhase(P, T, z, first, second, r);
+        }
+        if (r.converged)
+        {
+            canonicalizeFinal(P, T, r, true);
+            if (r.converged && !validatePhysical(P, T, z, r))
+                r.converged = false;
+        }
+    }
+
+    // flashRestrictedRecovery_ (restricted.inc:629-646)
+    __device__ void flashRestrictedRecovery(double P, double T, const double *zIn, uint8_t allowed, Result<NC> &r)
+    {
+        double z[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            z[i] = zIn[i];
+        normalize(z);
+        flashRestrictedImpl(P, T, z, allowed, nullptr, r);
+        if (r.converged)
+        {
+            canonicalizeFinal(P, T, r, false);
+            if (r.converged && !validatePhysical(P, T, z, r))
+                r.converged = false;
+        }
+    }
+
+    // stableReducedSetFallback_ (restricted.inc:655-693)
+    __device__ __noinline__ void stableReducedSetFallback(double P, double T, const double *z, Result<NC> &best)
+    {
+        best.init();
+        double bestG = __longlong_as_double(0x7ff0000000000000LL);
+        const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
+        Result<NC> cand;
+        for (int k = 0; k < 3; ++k)
+        {
+            flashRestrictedRecovery(P, T, z, pairs[k], cand);
+            if (err)
+                return;
+            if (!cand.converged)
+                continue;
+            cand.presence = presenceFromFractions(cand.beta);
+            if (cand.presence == 0)
+                continue;
+            StabilityResult<NC> st;
+            stabilityTest(P, T, z, cand.presence, cand.x, st);
+            if (!st.valid || !st.stable)
+                continue;
+            const double g = dimensionlessGibbs(P, T, cand);
+            if (isfinite(g) && g < bestG)
+            {
+                bestG = g;
+                best = cand;
+            }
+        }
+    }
+
+    // preferStableSwReducedOverSingle_ (restricted.inc:703-780)
+    __device__ __noinline__ void preferStableSwReducedOverSingle(double P, double T, const double *z,
+                                                                 Result<NC> &cand)
+    {
+        if (!sw() || popcount3(presenceFromFractions(cand.beta)) != 1)
+            return;
+        cand.presence = presenceFromFractions(cand.beta);
+        StabilityResult<NC> single;
+        stabilityTest(P, T, z, cand.presence, cand.x, single);
+        const bool singleKnownUnstable = single.valid && !single.stable;
+        Result<NC> reduced, trial;
+        reduced.init();
+        double reducedG = __longlong_as_double(0x7ff0000000000000LL);
+        const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
+        for (int k = 0; k < 3; ++k)
+        {
+            flashRestricted(P, T, z, pairs[k], nullptr, trial);
+            if (err)
+                return;
+            if (!trial.converged)
+                continue;
+            trial.presence = presenceFromFractions(trial.beta);
+            if (trial.presence == 0)
+                continue;
+            StabilityResult<NC> st;
+            stabilityTest(P, T, z, trial.presence, trial.x, st);
+            if (!st.valid || !st.stable)
+                continue;
+            const double g = dimensionlessGibbs(P, T, trial);
+            if (isfinite(g) && g < reducedG)
+            {
+                reducedG = g;
+                reduced = trial;
+            }
+        }
+        if (!reduced.converged)
+        {
+            if (singleKnownUnstable)
+                cand.converged = false;
+            return;
+        }
+        const double candG = dimensionlessGibbs(P, T, cand);
+        const double scale = smax3(1.0, fabs(candG), fabs(reducedG));
+        if (isfinite(reducedG) && (!isfinite(candG) || reducedG < candG - 1.0e-12 * scale))
+        {
+            cand = reduced;
+            return;
+        }
+        if (singleKnownUnstable)
+            cand.converged = false;
+    }
+
+    // numericalSwRoleResult_ (restricted.inc:514-541)
+    __device__ void numericalSwRoleResult(const Result<NC> &c, Result<NC> &n) const
+    {
+        n = c;
+        if (!sw())
+            return;
+        for (int p = 0; p < 3; ++p)
+        {
+            n.beta[p] = 0.0;
+            n.sat[p] = 0.0;
+            n.Z[p] = 1.0;
+            n.rho[p] = 0.0;
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                n.x[p][i] = 0.0;
+        }
+        for (int s = 0; s < 3; ++s)
+        {
+            const int phys = roles[s];
+            n.beta[s] = c.beta[phys];
+            n.sat[s] = c.sat[phys];
+            n.Z[s] = c.Z[phys];
+            n.rho[s] = c.rho[phys];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                n.x[s][i] = c.x[phys][i];
+        }
+        n.presence = presenceFromFractions(n.beta);
+        deriveReferenceK(n);
+    }
+
+    // --------------------------------------------------------------- flash --
+    // flash (three_phase_flash.hpp:83-227).  The nested solvers of the
+    // role-permutation search and the pressure continuation run with both
+    // recoveries disabled, exactly like the reference (core.inc:47-57).
+    template <bool TopLevel>
+    __device__ __noinline__ void flash(double P, double T, const double *zIn, Result<NC> &out)
+    {
+        out.init();
+        if (!validatePT(P, T))
+            return;
+        double z[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            z[i] = zIn[i];
+        normalize(z);
+        if (err)
+            return;
+        double kg[NC], kw[NC];
+        wilsonK(P, T, kg);
+        initialWaterK(kw);
+
+        Result<NC> seed;
+        flashTwo(P, T, z, OIL, GAS, kg, seed);
+        uint8_t active = presenceFromFractions(seed.beta);
+        if (!seed.converged || active == 0)
+        {
+            active = chooseSinglePhase(P, T, z);
+            singlePhaseResult(P, T, z, active, seed);
+        }
+        if (err)
+            return;
+        Result<NC> &selected = out;
+        equilibrateActiveSet(P, T, z, active, seed, true, selected);
+        if (err)
+            return;
+        if (selected.converged)
+        {
+            canonicalizeFinal(P, T, selected, false);
+            if (selected.converged && validatePhysical(P, T, z, selected))
+            {
+                Result<NC> preferred = selected;
+                preferStableSwReducedOverSingle(P, T, z, preferred);
+                if (preferred.converged)
+                {
+                    out = preferred;
+                    return;
+                }
+            }
+            selected.converged = false;
+        }
+        if (err)
+            return;
+        // recovery 1: direct three-phase solve
+        {
+            Result<NC> full;
+            flashThree(P, T, z, kg, kw, full);
+            if (full.converged)
+            {
+                canonicalize(P, T, full);
+                canonicalizeFinal(P, T, full, false);
+                if (full.converged && validatePhysical(P, T, z, full))
+                {
+                    preferStableSwReducedOverSingle(P, T, z, full);
+                    if (full.converged)
+                    {
+                        out = full;
+                        return;
+                    }
+                }
+            }
+        }
+        if (err)
+            return;
+        // recovery 2: stable reduced phase sets
+        {
+            Result<NC> reduced;
+            stableReducedSetFallback(P, T, z, reduced);
+            if (reduced.converged)
+            {
+                canonicalizeFinal(P, T, reduced, false);
+                if (reduced.converged && validatePhysical(P, T, z, reduced))
+                {
+                    out = reduced;
+                    return;
+                }
+            }
+        }
+        if (err)
+            return;
+        if (sw())
+        {
+            // recovery 3 (SW only): exact-mass allocation basin search -- not carried.
+            fail(ERR_NOT_PORTED);
+            return;
+        }
+        if (TopLevel && continuation)
+        {
+            Result<NC> continued;
+            pressureContinuation(P, T, z, continued);
+            if (continued.converged)
+            {
+                canonicalizeFinal(P, T, continued, false);
+                if (continued.converged && validatePhysical(P, T, z, continued))
+                {
+                    preferStableSwReducedOverSingle(P, T, z, continued);
+                    if (continued.converged)
+                    {
+                        out = continued;
+                        return;
+                    }
+                }
+            }
+        }
+    }
+
+    // pressureContinuationFallback_ (restricted.inc:554-627)
+    __device__ __noinline__ void pressureContinuation(double P, double T, const double *z, Result<NC> &out)
+    {
+        out.init();
+        if (!(P > 0.0))
+            return;
+        const double ratios[8] = {0.95, 1.05, 0.90, 1.10, 0.80, 1.25, 0.65, 1.50};
+        const double logTarget = log(P);
+        Result<NC> anchor, seed, current;
+#pragma unroll 1
+        for (int a = 0; a < 8; ++a)
+        {
+            const double anchorP = P * ratios[a];
+            if (!(anchorP > 0.0) || !isfinite(anchorP))
+                continue;
+            {
+                Solver<NC> nested = *this;
+                nested.permutationSearch = false;
+                nested.continuation = false;
+                nested.template flash<false>(anchorP, T, z, anchor);
+                evals = nested.evals;
+                if (nested.err)
+                {
+                    fail(nested.err);
+                    return;
+                }
+            }
+            if (!anchor.converged)
+                continue;
+            numericalSwRoleResult(anchor, seed);
+            if (!seed.converged || seed.presence == 0)
+                continue;
+            const double logAnchor = log(anchorP);
+            const double logSpan = fabs(logTarget - logAnchor);
+            int steps = int(ceil(logSpan / 0.025));
+            steps = steps < 1 ? 1 : (steps > 12 ? 12 : steps);
+            int totalIterations = anchor.iterations;
+            bool pathConverged = true;
+#pragma unroll 1
+            for (int s = 1; s <= steps; ++s)
+            {
+                const double fraction = double(s) / steps;
+                const double stepP = exp(logAnchor + fraction * (logTarget - logAnchor));
+                equilibrateActiveSet(stepP, T, z, seed.presence, seed, false, current);
+                if (err)
+                    return;
+                if (!current.converged)
+                {
+                    pathConverged = false;
+                    break;
+                }
+                totalIterations += current.iterations;
+                seed = current;
+            }
+            if (pathConverged && seed.converged)
+            {
+                seed.iterations = totalIterations;
+                out = seed;
+                return;
+            }
+        }
+    }
+};
+
+} // namespace nz

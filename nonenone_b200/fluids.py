@@ -1,0 +1,87 @@
+"""Fluid descriptions of the benchmark workloads.
+
+Component constants and where each comes from:
+
+* H2O / CO2 / nC10 (nc=3): Tc, Pc, omega and the three BIPs are the synthetic
+  set of the benchmark definition (H2O 647.1 K, 22.064 MPa, 0.344; CO2
+  304.13 K, 7.377 MPa, 0.225; nC10 617.7 K, 2.11 MPa, 0.49; k = 0.19 / 0.48 /
+  0.10).  Molar masses and critical volumes (needed by LBC viscosity) are the
+  reference case's (case/h2o_co2_nc10_2d_benchmark/case_config.hpp:53-58).
+  nC10 omega is exactly 0.49, so the strict PR78 switch ``omega > 0.49``
+  (models/include/natural/thermo/cubic_eos.hpp:606-613) keeps standard PR m.
+* C1, nC4 (case/three_eos_3d_compare/case_config.hpp:142-160), nC16
+  (case/scw_co2_nc4_nc16_3d_migration/case_config.hpp:46-55), C2, C3
+  (tools/example/pr_c2_c3_nc5/main.cpp:32-36).  BIPs not given by a reference
+  case are zero.
+"""
+from __future__ import annotations
+
+import math
+
+from .abi import (EOS_PR, EOS_SW, FluidDesc, MAX_NC, SW_BIP_CO2,
+                  SW_BIP_HYDROCARBON, SW_BIP_KIJ)
+
+OMEGA_A = 0.4572355
+OMEGA_B = 0.0779691
+M1 = 1.0 + math.sqrt(2.0)
+M2 = 1.0 - math.sqrt(2.0)
+
+# name: (Tc K, Pc Pa, Vc m3/mol, omega, Mw kg/mol)
+COMPONENTS = {
+    "H2O": (647.1, 22.064e6, 5.5948e-5, 0.344, 0.018015268),
+    "CO2": (304.13, 7.377e6, 9.4118e-5, 0.225, 0.0440098),
+    "nC10": (617.7, 2.11e6, 6.10e-4, 0.49, 0.14228168),
+    "C1": (190.564002651, 4.599200474e6, 9.862771707e-5, 0.01142, 0.0160428),
+    "C2": (305.32, 4.872e6, 1.458e-4, 0.099, 0.03007),
+    "C3": (369.83, 4.248e6, 2.000e-4, 0.152, 0.04410),
+    "nC4": (425.125, 3.796000017e6, 2.549219298e-4, 0.200810094644, 0.0581222),
+    "nC16": (723.0, 1.410e6, 9.0e-4, 0.742, 0.2264412),
+}
+
+# Symmetric pair BIPs; unlisted pairs are zero.
+PAIR_BIPS = {
+    frozenset(("H2O", "CO2")): 0.19,
+    frozenset(("H2O", "nC10")): 0.48,
+    frozenset(("CO2", "nC10")): 0.10,
+    frozenset(("H2O", "C1")): 0.4850,
+    frozenset(("H2O", "C2")): 0.5000,
+    frozenset(("H2O", "nC4")): 0.5000,
+    frozenset(("H2O", "nC16")): 0.5000,
+    frozenset(("CO2", "C1")): 0.1000,
+    frozenset(("CO2", "C2")): 0.1300,
+    frozenset(("CO2", "nC4")): 0.1277,
+    frozenset(("CO2", "nC16")): 0.0900,
+    frozenset(("C1", "nC4")): 0.09281,
+}
+
+H2O_CO2_NC10 = ("H2O", "CO2", "nC10")
+SIX_COMPONENT = ("H2O", "CO2", "C1", "nC4", "nC10", "nC16")
+
+
+def make_fluid(names=H2O_CO2_NC10, eos_model: int = EOS_PR, eos_type: int = 1,
+               salinity: float = 0.0) -> FluidDesc:
+    """Build an nz_fluid_desc.  H2O must be present; it is the water component."""
+    nc = len(names)
+    if not 2 <= nc <= MAX_NC:
+        raise ValueError("nc must be in 2..8")
+    d = FluidDesc()
+    d.nc = nc
+    d.eos_model = eos_model
+    d.eos_type = eos_type
+    d.water_component = names.index("H2O") if "H2O" in names else -1
+    d.omega_a, d.omega_b, d.m1, d.m2 = OMEGA_A, OMEGA_B, M1, M2
+    d.minimum_composition = 1.0e-8
+    for i, n in enumerate(names):
+        tc, pc, vc, om, mw = COMPONENTS[n]
+        d.tc[i], d.pc[i], d.vc[i], d.acentric[i], d.mw[i] = tc, pc, vc, om, mw
+        for j, m in enumerate(names):
+            if i != j:
+                d.kij[i * MAX_NC + j] = PAIR_BIPS.get(frozenset((n, m)), 0.0)
+    d.sw_salinity = salinity
+    for i, n in enumerate(names):
+        if eos_model == EOS_SW and n != "H2O":
+            # Aqueous BIP correlations of the SW model (soreide_whitson.hpp:54-134)
+            d.sw_bip_kind[i] = SW_BIP_CO2 if n == "CO2" else SW_BIP_HYDROCARBON
+        else:
+            d.sw_bip_kind[i] = SW_BIP_KIJ
+    return d

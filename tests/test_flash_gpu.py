@@ -1,0 +1,186 @@
+"""GPU flash / EOS / stability parity against the reference oracle.
+
+Tolerances (from the benchmark definition):
+  * status and phase labels bit-exact, except points within |trialSum-1| < 1e-8
+    of a phase boundary (or with a phase fraction < 1e-8), counted and bounded;
+  * phase fractions and compositions within 1e-8 (relative, scale max(1,|v|));
+  * EOS Z / ln phi within 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from nonenone_b200 import abi
+from nonenone_b200.fluids import SIX_COMPONENT, make_fluid
+from tests import kat
+
+pytestmark = pytest.mark.gpu
+
+BOUNDARY_TPD = 1e-8
+BOUNDARY_BETA = 1e-8
+VALUE_TOL = 1e-8
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a visible CUDA device")
+    return torch
+
+
+def _np(d):
+    return {k: v.cpu().numpy() for k, v in d.items()}
+
+
+def _near_boundary(g):
+    beta = g["beta"]
+    present = np.stack([(g["presence"] >> p) & 1 for p in range(3)]).astype(bool)
+    small = np.any(present & (beta < BOUNDARY_BETA), axis=0)
+    return (g["tpd_distance"] < BOUNDARY_TPD) | small
+
+
+def compare_flash(gpu, g, max_boundary_fraction=0.02):
+    n = g["P"].shape[0]
+    boundary = _near_boundary(g)
+    same_status = gpu["status"] == g["status"]
+    same_label = gpu["presence"] == g["presence"]
+    bad = ~(same_status & same_label) & ~boundary
+    assert not bad.any(), (
+        f"{bad.sum()} label/status mismatches away from phase boundaries: idx {np.where(bad)[0][:10]}, "
+        f"gpu {gpu['presence'][bad][:10]} ref {g['presence'][bad][:10]} "
+        f"gpu status {gpu['status'][bad][:10]} ref {g['status'][bad][:10]}")
+    mism = ~(same_status & same_label)
+    assert mism.sum() <= max_boundary_fraction * n
+    ok = same_status & same_label & (g["status"] == abi.FLASH_CONVERGED)
+    for key in ("beta", "composition"):
+        a, b = gpu[key][..., ok], g[key][..., ok]
+        err = np.abs(a - b) / np.maximum(1.0, np.abs(b))
+        assert err.max() <= VALUE_TOL, (key, err.max(), np.unravel_index(err.argmax(), err.shape))
+    present = np.stack([(g["presence"] >> p) & 1 for p in range(3)]).astype(bool) & ok
+    for key in ("saturation", "compressibility", "molar_density"):
+        # absent slots carry no physical value (the reference leaves stale entries)
+        a, b = gpu[key][present], g[key][present]
+        err = np.abs(a - b) / np.maximum(1.0, np.abs(b))
+        assert err.max() <= 1e-7, (key, err.max())
+    return int(mism.sum())
+
+
+def test_eos_kat_on_gpu(torch_cuda):
+    from nonenone_b200.flash import CubicEquationOfState
+    eos = CubicEquationOfState(kat.eos6_fluid())
+    P = np.full(2, kat.EOS6_P)
+    T = np.full(2, kat.EOS6_T)
+    x = np.stack([kat.EOS6_X, kat.EOS6_Y], axis=1)
+    Z, lnphi = eos.phase_result(P, T, x, np.array([abi.OIL, abi.GAS], np.int8))
+    Z, lnphi = Z.cpu().numpy(), lnphi.cpu().numpy()
+    assert kat.near(Z[0], kat.EOS6_ZL, 2e-12) and kat.near(Z[1], kat.EOS6_ZV, 2e-12)
+    assert kat.near(np.exp(lnphi[:, 0]) * kat.EOS6_X * kat.EOS6_P, kat.EOS6_FL, 2e-8)
+    assert kat.near(np.exp(lnphi[:, 1]) * kat.EOS6_Y * kat.EOS6_P, kat.EOS6_FV, 2e-8)
+
+
+@pytest.mark.parametrize("eos_model", [abi.EOS_PR, abi.EOS_SW])
+def test_eos_matches_reference_random(torch_cuda, reference, eos_model):
+    from nonenone_b200.flash import CubicEquationOfState
+    f = make_fluid(eos_model=eos_model)
+    rng = np.random.default_rng(7)
+    n = 3000
+    P = rng.uniform(1e6, 60e6, n)
+    T = rng.uniform(290, 450, n)
+    x = np.ascontiguousarray(rng.dirichlet([1, 1, 1], n).T)
+    role = rng.integers(0, 3, n).astype(np.int8)
+    sal = rng.uniform(0, 2, n)
+    Zr, lr = reference.eos_phase_batch(f, P, T, x, role, salinity=sal)
+    eos = CubicEquationOfState(f)
+    Zg, lg = eos.phase_result(P, T, x, role, salinity=sal)
+    Zg, lg = Zg.cpu().numpy(), lg.cpu().numpy()
+    assert np.array_equal(np.isfinite(Zr), np.isfinite(Zg))
+    m = np.isfinite(Zr)
+    assert kat.near(Zg[m], Zr[m], 1e-12)
+    assert kat.near(lg[:, m], lr[:, m], 1e-11)
+
+
+def test_flash_three_phase_kat_on_gpu(torch_cuda):
+    from nonenone_b200.flash import CubicEquationOfState, CubicThreePhaseFlash
+    f = kat.flash4_fluid()
+    fl = CubicThreePhaseFlash(f)
+    out = _np(fl.flash([kat.FLASH4_P], [kat.FLASH4_T], kat.FLASH4_Z.reshape(4, 1)))
+    assert out["status"][0] == 0 and out["presence"][0] == 7
+    comp = out["composition"][:, :, 0]
+    eos = CubicEquationOfState(f)
+    Z, lnphi = eos.phase_result(np.full(3, kat.FLASH4_P), np.full(3, kat.FLASH4_T),
+                                comp.T.copy(), np.array([0, 1, 2], np.int8))
+    lnphi = lnphi.cpu().numpy()
+    fug = [np.exp(lnphi[:, p]) * comp[p] * kat.FLASH4_P for p in range(3)]
+    kat.check_flash4(out["beta"][:, 0], out["saturation"][:, 0], comp, Z.cpu().numpy(), *fug)
+
+
+@pytest.mark.parametrize("name,fluid_args", [
+    ("flash_pr_nc3.npz", dict()),
+    ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
+    ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
+])
+def test_flash_matches_golden(torch_cuda, golden, name, fluid_args):
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    g = golden(name)
+    fl = CubicThreePhaseFlash(make_fluid(**fluid_args))
+    out = _np(fl.flash(g["P"], g["T"], g["z"], salinity=g.get("salinity")))
+    compare_flash(out, g)
+
+
+def test_flash_matches_reference_fresh_sample(torch_cuda, reference):
+    """A fresh seeded sample of the batched-flash workload, oracle run live."""
+    from nonenone_b200 import synth
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    from tests.golden.make_golden import boundary_distance
+    f = make_fluid()
+    P, T, z = synth.flash_points(4096, seed=2024)
+    r = reference.flash_batch(f, P, T, z, threads=8)
+    r["tpd_distance"] = boundary_distance(f, P, T, z, r)
+    r.update(P=P, T=T, z=z)
+    out = _np(CubicThreePhaseFlash(f).flash(P, T, z))
+    compare_flash(out, r)
+
+
+def test_flash_edge_cases(torch_cuda, reference):
+    """Empty batch, invalid P/T/z and a pure-water feed behave like the reference."""
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    f = make_fluid()
+    fl = CubicThreePhaseFlash(f)
+    out = fl.flash(np.zeros(0), np.zeros(0), np.zeros((3, 0)))
+    assert out["status"].numel() == 0
+    P = np.array([-1.0, 1e7, 1e7, np.nan, 1e7, 2e7])
+    T = np.array([350.0, 0.0, 350.0, 350.0, 350.0, 360.0])
+    z = np.array([[0.5, 0.5, np.nan, 0.5, 1.0, 1 - 1e-9],
+                  [0.3, 0.3, 0.3, 0.3, 0.0, 5e-10],
+                  [0.2, 0.2, 0.2, 0.2, 0.0, 5e-10]])
+    g = _np(fl.flash(P, T, z))
+    r = reference.flash_batch(f, P, T, z)
+    assert np.array_equal(g["status"], r["status"])
+    assert np.array_equal(g["presence"], r["presence"])
+
+
+def test_flash_host_entry_point_equals_device(torch_cuda, golden):
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    g = golden("flash_pr_nc3.npz")
+    fl = CubicThreePhaseFlash(make_fluid())
+    d = _np(fl.flash(g["P"], g["T"], g["z"]))
+    h = fl.flash_host(g["P"], g["T"], g["z"])
+    for k in ("status", "presence", "beta", "composition", "saturation", "k_gas_oil"):
+        assert np.array_equal(d[k], h[k]), k
+
+
+def test_stability_matches_reference(torch_cuda, reference, golden):
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    g = golden("flash_pr_nc3.npz")
+    f = make_fluid()
+    ok = (g["status"] == 0) & (g["presence"] != 7)
+    idx = np.where(ok)[0][:600]
+    args = (g["P"][idx], g["T"][idx], g["z"][:, idx], g["presence"][idx], g["composition"][:, :, idx])
+    r = reference.stability_batch(f, *args)
+    s = {k: v.cpu().numpy() for k, v in CubicThreePhaseFlash(f).stability_test(*args).items()}
+    assert np.array_equal(s["valid"], r["valid"])
+    near = np.abs(r["trial_sum"] - 1.0).min(axis=0) < BOUNDARY_TPD
+    assert np.array_equal(s["stable"][~near], r["stable"][~near])
+    miss = np.stack([((g["presence"][idx] >> p) & 1) == 0 for p in range(3)])
+    err = np.abs(s["trial_sum"] - r["trial_sum"])[miss]
+    assert err.max() < 1e-7
