@@ -15,8 +15,42 @@
 #include <cstdint>
 #include <math.h>
 
+// Device code is CUDA; the same headers also compile as plain C++ so that a
+// host build can be used to step through a point when debugging.
+#ifdef __CUDACC__
+#define NZ_HD __device__
+#define NZ_HDI __device__ __forceinline__
+#define NZ_HDN __device__ __noinline__
+#else
+#include <cmath>
+#include <cstring>
+using std::isfinite;
+#define NZ_HD
+#define NZ_HDI inline
+#define NZ_HDN __attribute__((noinline))
+#endif
+
 namespace nz
 {
+
+NZ_HDI double nzNan()
+{
+#ifdef __CUDACC__
+    return __longlong_as_double(0x7ff8000000000000LL);
+#else
+    return std::nan("");
+#endif
+}
+NZ_HDI double nzInf()
+{
+#ifdef __CUDACC__
+    return __longlong_as_double(0x7ff0000000000000LL);
+#else
+    return HUGE_VAL;
+#endif
+}
+NZ_HDI int imin(int a, int b) { return a < b ? a : b; }
+NZ_HDI int imax(int a, int b) { return a < b ? b : a; }
 
 constexpr double kGasConstant = 8.31446261815324;   // common/units.hpp
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -39,21 +73,21 @@ constexpr int ERR_EOS = 3;         // std::runtime_error in the reference
 constexpr int ERR_NOT_PORTED = 4;
 
 // std::max / std::min / std::clamp with the same NaN behaviour as libstdc++.
-__host__ __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
-__host__ __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
-__host__ __device__ __forceinline__ double smax3(double a, double b, double c)
+NZ_HDI double smax(double a, double b) { return (a < b) ? b : a; }
+NZ_HDI double smin(double a, double b) { return (b < a) ? b : a; }
+NZ_HDI double smax3(double a, double b, double c)
 {
     double r = a;
     if (r < b) r = b;
     if (r < c) r = c;
     return r;
 }
-__host__ __device__ __forceinline__ double sclamp(double v, double lo, double hi)
+NZ_HDI double sclamp(double v, double lo, double hi)
 {
     return (v < lo) ? lo : ((hi < v) ? hi : v);
 }
-__host__ __device__ __forceinline__ int bitOf(int slot) { return 1 << slot; }
-__host__ __device__ __forceinline__ int popcount3(uint8_t b)
+NZ_HDI int bitOf(int slot) { return 1 << slot; }
+NZ_HDI int popcount3(uint8_t b)
 {
     return (b & 1) + ((b >> 1) & 1) + ((b >> 2) & 1);
 }
@@ -112,7 +146,7 @@ struct PhaseMix
 };
 
 // ---- Soreide-Whitson correlations (soreide_whitson.hpp) -------------------
-__device__ __forceinline__ double swWaterAlpha(double T, double tcw, double salinity)
+NZ_HDI double swWaterAlpha(double T, double tcw, double salinity)
 {
     const double tr = T / tcw;
     const double saltFactor = 1.0 - 0.0103 * pow(salinity, 1.1);
@@ -121,7 +155,7 @@ __device__ __forceinline__ double swWaterAlpha(double T, double tcw, double sali
     return sqrtAlpha * sqrtAlpha;
 }
 
-__device__ __forceinline__ double swHydrocarbonBip(double T, double tc, double omega, double s)
+NZ_HDI double swHydrocarbonBip(double T, double tc, double omega, double s)
 {
     const double tr = T / tc;
     const double a0 = 1.1120 - 1.7369 * pow(omega, -0.1);
@@ -132,7 +166,7 @@ __device__ __forceinline__ double swHydrocarbonBip(double T, double tc, double o
         + a2 * tr * tr * (1.0 + alpha2 * s);
 }
 
-__device__ __forceinline__ double swCo2Bip(double T, double tc, double s)
+NZ_HDI double swCo2Bip(double T, double tc, double s)
 {
     const double tr = T / tc;
     return -0.31092 * (1.0 + 0.15587 * pow(s, 0.7505))
@@ -140,7 +174,7 @@ __device__ __forceinline__ double swCo2Bip(double T, double tc, double s)
         - 21.2566 * exp(-6.7222 * tr - s);
 }
 
-__device__ __forceinline__ double swCo2BipChabab(double T, double s)
+NZ_HDI double swCo2BipChabab(double T, double s)
 {
     const double tr = T / 304.13;
     const double a = 0.43575155, b = -0.05766906744, c = 0.00826464849;
@@ -149,7 +183,7 @@ __device__ __forceinline__ double swCo2BipChabab(double T, double s)
 }
 
 // soreideWhitsonAqueousBip_ (cubic_eos.hpp:2389-2404)
-__device__ __forceinline__ double swAqueousBip(const FluidDev &F, int i, int j, double T, double s)
+NZ_HDI double swAqueousBip(const FluidDev &F, int i, int j, double T, double s)
 {
     const int w = F.water;
     if (i != w && j != w)
@@ -169,7 +203,7 @@ __device__ __forceinline__ double swAqueousBip(const FluidDev &F, int i, int j, 
 
 // mixingParameters(P, T, role) (cubic_eos.hpp:581-650)
 template <int NC>
-__device__ void mixingParameters(const FluidDev &F, double P, double T, double salinity,
+NZ_HD void mixingParameters(const FluidDev &F, double P, double T, double salinity,
                                  bool aqueousRole, MixParams<NC> &out)
 {
     double sqrtAi[NC];
@@ -216,7 +250,7 @@ __device__ void mixingParameters(const FluidDev &F, double P, double T, double s
 
 // phaseMixing (cubic_eos.hpp:666-692)
 template <int NC>
-__device__ __forceinline__ void phaseMixing(const double *x, const MixParams<NC> &p, PhaseMix<NC> &m)
+NZ_HDI void phaseMixing(const double *x, const MixParams<NC> &p, PhaseMix<NC> &m)
 {
     m.A = 0.0;
     m.B = 0.0;
@@ -237,7 +271,7 @@ __device__ __forceinline__ void phaseMixing(const double *x, const MixParams<NC>
 
 // solveCubic + liquid/vapour root choice (cubic_eos.hpp:696-803).
 // Returns the selected root or NaN (the reference throws) when none has Z > B.
-__device__ __forceinline__ double selectCubicRoot(double A, double B, double m1, double m2, bool vapour)
+NZ_HDI double selectCubicRoot(double A, double B, double m1, double m2, bool vapour)
 {
     const double e0 = -(A * B + m1 * m2 * B * B * (B + 1.0));
     const double e1 = A - (m1 + m2 - m1 * m2) * B * B - (m1 + m2) * B;
@@ -246,7 +280,7 @@ __device__ __forceinline__ double selectCubicRoot(double A, double B, double m1,
     const double Q = (a * a - 3.0 * b) / 9.0;
     const double R = (2.0 * a * a * a - 9.0 * a * b + 27.0 * c) / 54.0;
     const double disc = R * R - Q * Q * Q;
-    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    const double nan = nzNan();
     double r0 = nan, r1 = nan, r2 = nan;
     if (disc < 0.0)
     {
@@ -297,7 +331,7 @@ __device__ __forceinline__ double selectCubicRoot(double A, double B, double m1,
 // fugacityAtRoot (cubic_eos.hpp:902-934): phi_i = exp(ln phi_i).
 // Returns false where the reference throws.
 template <int NC>
-__device__ __forceinline__ bool fugacityCoefficients(const double *x, const MixParams<NC> &p,
+NZ_HDI bool fugacityCoefficients(const double *x, const MixParams<NC> &p,
                                                      const PhaseMix<NC> &m, double Z,
                                                      double m1, double m2, double *phi)
 {
@@ -321,7 +355,7 @@ __device__ __forceinline__ bool fugacityCoefficients(const double *x, const MixP
 }
 
 // molarDensity without volume translation (cubic_eos.hpp:511-523)
-__device__ __forceinline__ double molarDensity(double P, double T, double Z)
+NZ_HDI double molarDensity(double P, double T, double Z)
 {
     return P / (kGasConstant * T * Z);
 }

@@ -14,9 +14,8 @@
 //  * the SSI steps of the TPD trial reuse the fugacity coefficients of the
 //    residual evaluation at the same composition (the reference evaluates
 //    the EOS twice there; the EOS is deterministic so the values are equal);
-//  * the Soreide-Whitson exact-mass allocation recovery
-//    (three_phase_flash_allocation.inc:609-700) is not carried: a point that
-//    reaches it returns NZ_FLASH_NOT_PORTED.
+//  * a restricted flash asked for all three phases (never requested by the
+//    entry points carried here) returns NZ_FLASH_NOT_PORTED.
 #pragma once
 
 #include "eos.cuh"
@@ -38,7 +37,7 @@ struct Result
     double Kg[NC];
     double Kw[NC];
 
-    __device__ void init()
+    NZ_HD void init()
     {
         converged = false;
         iterations = 0;
@@ -111,12 +110,12 @@ struct ThreePhaseLogKState
 };
 
 // ---- small helpers ---------------------------------------------------------
-__device__ __forceinline__ int firstActive(uint8_t b)
+NZ_HDI int firstActive(uint8_t b)
 {
     return (b & OIL_BIT) ? OIL : ((b & GAS_BIT) ? GAS : WATER);
 }
 
-__device__ __forceinline__ void activePair(uint8_t b, int &first, int &second)
+NZ_HDI void activePair(uint8_t b, int &first, int &second)
 {
     int n = 0;
     first = OIL;
@@ -134,7 +133,7 @@ __device__ __forceinline__ void activePair(uint8_t b, int &first, int &second)
 
 // Dense Gaussian elimination with partial pivoting (stability.inc:98-146).
 template <int M>
-__device__ bool solveDense(double (&m)[M][M], double (&rhs)[M], double (&sol)[M])
+NZ_HD bool solveDense(double (&m)[M][M], double (&rhs)[M], double (&sol)[M])
 {
 #pragma unroll 1
     for (int k = 0; k < M; ++k)
@@ -192,7 +191,7 @@ __device__ bool solveDense(double (&m)[M][M], double (&rhs)[M], double (&sol)[M]
 }
 
 // The SW role permutations (core.inc:37-45).
-__device__ __forceinline__ void swRolePermutation(int k, int (&roles)[3])
+NZ_HDI void swRolePermutation(int k, int (&roles)[3])
 {
     const int table[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
     roles[0] = table[k][0];
@@ -217,7 +216,7 @@ struct Solver
     MixParams<NC> nonAq;
     MixParams<NC> aq;
 
-    __device__ void setup(const FluidDev *fluid, double s)
+    NZ_HD void setup(const FluidDev *fluid, double s)
     {
         F = fluid;
         salinity = s;
@@ -230,19 +229,19 @@ struct Solver
         cacheP = cacheT = 0.0;
     }
 
-    __device__ const FlashOpts &O() const { return F->opt; }
-    __device__ bool sw() const { return F->eosModel == EOS_SW; }
+    NZ_HD const FlashOpts &O() const { return F->opt; }
+    NZ_HD bool sw() const { return F->eosModel == EOS_SW; }
 
-    __device__ void fail(int code)
+    NZ_HD void fail(int code)
     {
         if (err == ERR_NONE)
             err = code;
     }
 
     // ---------------------------------------------------------------- core --
-    __device__ int thermodynamicRole(int slot) const { return sw() ? roles[slot] : slot; }
+    NZ_HD int thermodynamicRole(int slot) const { return sw() ? roles[slot] : slot; }
 
-    __device__ void ensureCache(double P, double T)
+    NZ_HD void ensureCache(double P, double T)
     {
         if (cacheValid && cacheP == P && cacheT == T)
             return;
@@ -255,7 +254,7 @@ struct Solver
     }
 
     // phaseResultForThermodynamicRole_ (core.inc:101-126)
-    __device__ __noinline__ double phaseForRole(int role, double P, double T, const double *x, double *phi)
+    NZ_HDN double phaseForRole(int role, double P, double T, const double *x, double *phi)
     {
         ensureCache(P, T);
         const MixParams<NC> &p = (role == WATER && sw()) ? aq : nonAq;
@@ -266,7 +265,7 @@ struct Solver
         if (!isfinite(Z) || !fugacityCoefficients<NC>(x, p, m, Z, F->m1, F->m2, phi))
         {
             fail(ERR_EOS);
-            const double nan = __longlong_as_double(0x7ff8000000000000LL);
+            const double nan = nzNan();
 #pragma unroll
             for (int i = 0; i < NC; ++i)
                 phi[i] = nan;
@@ -275,12 +274,12 @@ struct Solver
         return Z;
     }
 
-    __device__ double phase(int slot, double P, double T, const double *x, double *phi)
+    NZ_HD double phase(int slot, double P, double T, const double *x, double *phi)
     {
         return phaseForRole(thermodynamicRole(slot), P, T, x, phi);
     }
 
-    __device__ bool validatePT(double P, double T)
+    NZ_HD bool validatePT(double P, double T)
     {
         if (!(P > 0.0) || !isfinite(P) || !(T > 0.0) || !isfinite(T))
         {
@@ -291,7 +290,7 @@ struct Solver
     }
 
     // normalize_ (core.inc:136-149)
-    __device__ void normalize(double *x)
+    NZ_HD void normalize(double *x)
     {
         double sum = 0.0;
 #pragma unroll
@@ -310,7 +309,7 @@ struct Solver
     }
 
     // wilsonGasOilK_ (core.inc:152-165)
-    __device__ void wilsonK(double P, double T, double *K) const
+    NZ_HD void wilsonK(double P, double T, double *K) const
     {
 #pragma unroll
         for (int i = 0; i < NC; ++i)
@@ -321,7 +320,7 @@ struct Solver
     }
 
     // initialWaterOilK_ (core.inc:168-176)
-    __device__ void initialWaterK(double *K) const
+    NZ_HD void initialWaterK(double *K) const
     {
 #pragma unroll
         for (int i = 0; i < NC; ++i)
@@ -329,7 +328,7 @@ struct Solver
         K[F->water >= 0 ? F->water : NC - 1] = 50.0;
     }
 
-    __device__ uint8_t presenceFromFractions(const double *beta) const
+    NZ_HD uint8_t presenceFromFractions(const double *beta) const
     {
         uint8_t b = 0;
         for (int p = 0; p < 3; ++p)
@@ -340,10 +339,10 @@ struct Solver
 
     // ------------------------------------------------------- Rachford-Rice --
     // residual/Jacobian of the three-phase RR (nonlinear.inc:30-58)
-    __device__ double rr3Norm(const double *z, const double *kg, const double *kw, double cg, double cw,
+    NZ_HD double rr3Norm(const double *z, const double *kg, const double *kw, double cg, double cw,
                               double &fg, double &fw, double &jgg, double &jww, double &jgw) const
     {
-        const double inf = __longlong_as_double(0x7ff0000000000000LL);
+        const double inf = nzInf();
         if (!(cg > 0.0) || !(cw > 0.0) || !(cg + cw < 1.0))
             return inf;
         fg = 0.0; fw = 0.0; jgg = 0.0; jww = 0.0; jgw = 0.0;
@@ -367,7 +366,7 @@ struct Solver
     }
 
     // solveRr3_ (nonlinear.inc:8-96)
-    __device__ bool rr3(const double *z, const double *kg, const double *kw, double initBg, double initBw,
+    NZ_HD bool rr3(const double *z, const double *kg, const double *kw, double initBg, double initBw,
                         double &outBg, double &outBw) const
     {
         double bg = sclamp(initBg, 1.0e-4, 0.8);
@@ -421,7 +420,7 @@ struct Solver
     }
 
     // solveRr3Robust_ (nonlinear.inc:98-127)
-    __device__ bool rr3Robust(const double *z, const double *kg, const double *kw, double pg, double pw,
+    NZ_HD bool rr3Robust(const double *z, const double *kg, const double *kw, double pg, double pw,
                               double &bg, double &bw) const
     {
         const double guesses[17][2] = {
@@ -437,7 +436,7 @@ struct Solver
     }
 
     // solveRr2_ (nonlinear.inc:129-187)
-    __device__ double rr2Eval(const double *z, const double *K, double beta, double &df) const
+    NZ_HD double rr2Eval(const double *z, const double *K, double beta, double &df) const
     {
         double f = 0.0;
         df = 0.0;
@@ -447,14 +446,14 @@ struct Solver
             const double a = K[i] - 1.0;
             const double D = (1.0 - beta) + beta * K[i];
             if (!(D > 1.0e-300) || !isfinite(D))
-                return __longlong_as_double(0x7ff8000000000000LL);
+                return nzNan();
             f += z[i] * a / D;
             df -= z[i] * a * a / (D * D);
         }
         return f;
     }
 
-    __device__ bool rr2(const double *z, const double *K, double initialBeta, double &out) const
+    NZ_HD bool rr2(const double *z, const double *K, double initialBeta, double &out) const
     {
         double d0;
         const double f0 = rr2Eval(z, K, 0.0, d0);
@@ -498,7 +497,7 @@ struct Solver
 
     // ----------------------------------------------------- result helpers --
     // deriveReferenceK_ (restricted.inc:414-423)
-    __device__ void deriveReferenceK(Result<NC> &r) const
+    NZ_HD void deriveReferenceK(Result<NC> &r) const
     {
 #pragma unroll
         for (int i = 0; i < NC; ++i)
@@ -511,7 +510,7 @@ struct Solver
 
     // updateSaturationsFromMoles (three_phase_flash.hpp:527-575).  No aqueous
     // volume closure is configured, so every Water composition is admissible.
-    __device__ void updateSaturations(double P, double T, Result<NC> &r)
+    NZ_HD void updateSaturations(double P, double T, Result<NC> &r)
     {
         double volumeSum = 0.0;
         double volume[3] = {0.0, 0.0, 0.0};
@@ -545,7 +544,7 @@ struct Solver
     }
 
     // singlePhaseResult_ (restricted.inc:425-447)
-    __device__ void singlePhaseResult(double P, double T, const double *z, uint8_t active, Result<NC> &r)
+    NZ_HD void singlePhaseResult(double P, double T, const double *z, uint8_t active, Result<NC> &r)
     {
         r.init();
         r.converged = true;
@@ -568,7 +567,7 @@ struct Solver
     }
 
     // waterIsDominant_ (canonicalization.inc:68-85)
-    __device__ bool waterIsDominant(const double *x) const
+    NZ_HD bool waterIsDominant(const double *x) const
     {
         if (F->water < 0)
             return false;
@@ -581,7 +580,7 @@ struct Solver
     }
 
     // chooseSinglePhase_ (restricted.inc:449-478)
-    __device__ uint8_t chooseSinglePhase(double P, double T, const double *z)
+    NZ_HD uint8_t chooseSinglePhase(double P, double T, const double *z)
     {
         double phi[NC];
         double g[3];
@@ -608,7 +607,7 @@ struct Solver
     }
 
     // dimensionlessGibbs_ (restricted.inc:480-505); the public slot is the role.
-    __device__ double dimensionlessGibbs(double P, double T, const Result<NC> &r)
+    NZ_HD double dimensionlessGibbs(double P, double T, const Result<NC> &r)
     {
         double g = 0.0;
         double phi[NC];
@@ -629,7 +628,7 @@ struct Solver
         return g;
     }
 
-    __device__ void swapSlots(Result<NC> &r, int a, int b) const
+    NZ_HD void swapSlots(Result<NC> &r, int a, int b) const
     {
         if (a == b)
             return;
@@ -647,7 +646,7 @@ struct Solver
 
     // ------------------------------------------------------- pair seeds ----
     // pairInitialK_ (nonlinear.inc:515-623)
-    __device__ void pairInitialK(int first, int second, double P, double T, const double *z, double *K)
+    NZ_HD void pairInitialK(int first, int second, double P, double T, const double *z, double *K)
     {
         if (sw() && (first == WATER || second == WATER))
         {
@@ -721,12 +720,12 @@ struct Solver
 
     // --------------------------------------------------------- two-phase ---
     // evaluateTwoPhaseLogK_ (restricted.inc:71-134)
-    __device__ __noinline__ void evalTwo(double P, double T, const double *z, int first, int second,
+    NZ_HDN void evalTwo(double P, double T, const double *z, int first, int second,
                                          const double *logK, double preferredSecond,
                                          TwoPhaseLogKState<NC> &s)
     {
         s.valid = false;
-        s.norm = __longlong_as_double(0x7ff0000000000000LL);
+        s.norm = nzInf();
         s.result.init();
         double K[NC];
 #pragma unroll
@@ -782,7 +781,7 @@ struct Solver
     }
 
     // one damped SSI step of flashTwo_ (restricted.inc:155-208)
-    __device__ bool twoSsiStep(double P, double T, const double *z, int first, int second, double *K,
+    NZ_HD bool twoSsiStep(double P, double T, const double *z, int first, int second, double *K,
                                double &betaSecond, int &totalIterations, Result<NC> &r)
     {
         double bS;
@@ -844,7 +843,7 @@ struct Solver
     }
 
     // flashTwo_ (restricted.inc:136-327)
-    __device__ __noinline__ void flashTwo(double P, double T, const double *z, int first, int second,
+    NZ_HDN void flashTwo(double P, double T, const double *z, int first, int second,
                                           const double *Kin, Result<NC> &r)
     {
         r.init();
@@ -855,7 +854,7 @@ struct Solver
             K[i] = sclamp(Kin[i], 1.0e-100, 1.0e100);
         double betaSecond = 0.5;
         int total = 0;
-        const int ssiSteps = min(O().maxIterations, max(O().twoSsi, 0));
+        const int ssiSteps = imin(O().maxIterations, imax(O().twoSsi, 0));
 #pragma unroll 1
         for (int it = 0; it < ssiSteps; ++it)
         {
@@ -958,7 +957,7 @@ struct Solver
     }
 
     // finalizePhysicallyConvergedTwoPhase_ (restricted.inc:336-412)
-    __device__ void finalizePhysicallyConvergedTwoPhase(double P, double T, const double *z, int first,
+    NZ_HD void finalizePhysicallyConvergedTwoPhase(double P, double T, const double *z, int first,
                                                         int second, Result<NC> &r)
     {
         if (r.converged)
@@ -1018,12 +1017,12 @@ struct Solver
 
     // ------------------------------------------------------- three-phase ---
     // evaluateThreePhaseLogK_ (nonlinear.inc:200-277)
-    __device__ __noinline__ void evalThree(double P, double T, const double *z, const double *logK,
+    NZ_HDN void evalThree(double P, double T, const double *z, const double *logK,
                                            double preferredGas, double preferredWater,
                                            ThreePhaseLogKState<NC> &s)
     {
         s.valid = false;
-        s.norm = __longlong_as_double(0x7ff0000000000000LL);
+        s.norm = nzInf();
         s.result.init();
         double kg[NC], kw[NC];
 #pragma unroll
@@ -1084,7 +1083,7 @@ struct Solver
     }
 
     // one damped SSI step of flashThree_ (nonlinear.inc:301-371)
-    __device__ bool threeSsiStep(double P, double T, const double *z, double *kg, double *kw,
+    NZ_HD bool threeSsiStep(double P, double T, const double *z, double *kg, double *kw,
                                  double &bg, double &bw, int &total, Result<NC> &r)
     {
         double ng, nw;
@@ -1149,7 +1148,7 @@ struct Solver
     }
 
     // flashThree_ (nonlinear.inc:279-513)
-    __device__ __noinline__ void flashThree(double P, double T, const double *z, const double *kgIn,
+    NZ_HDN void flashThree(double P, double T, const double *z, const double *kgIn,
                                             const double *kwIn, Result<NC> &r)
     {
         r.init();
@@ -1162,7 +1161,7 @@ struct Solver
             kw[i] = sclamp(kwIn[i], 1.0e-100, 1.0e100);
         }
         double bg = 0.15, bw = 0.15;
-        const int ssiSteps = min(O().maxIterations, max(O().threeSsi, 0));
+        const int ssiSteps = imin(O().maxIterations, imax(O().threeSsi, 0));
         int total = 0;
 #pragma unroll 1
         for (int it = 0; it < ssiSteps; ++it)
@@ -1288,7 +1287,7 @@ struct Solver
 
     // ----------------------------------------------------- stability -------
     // evaluateStabilityResidual_ (stability.inc:157-204)
-    __device__ void stabilityResidual(int candidate, double P, double T, const double *logRef,
+    NZ_HD void stabilityResidual(int candidate, double P, double T, const double *logRef,
                                       const double *logW, StabilityResidual<NC> &s)
     {
         s.valid = false;
@@ -1315,7 +1314,7 @@ struct Solver
         for (int i = 0; i < NC; ++i)
             s.x[i] /= scaledSum;
         const double logSum = maxLogW + log(scaledSum);
-        s.sum = logSum > 709.782712893384 ? __longlong_as_double(0x7ff0000000000000LL) : exp(logSum);
+        s.sum = logSum > 709.782712893384 ? nzInf() : exp(logSum);
         phase(candidate, P, T, s.x, s.phi);
         s.norm = 0.0;
 #pragma unroll
@@ -1331,7 +1330,7 @@ struct Solver
     }
 
     // finalizeStabilityTrial_ (stability.inc:206-223)
-    __device__ void finalizeTrial(const StabilityResidual<NC> &s, const double *ref, Trial<NC> &t) const
+    NZ_HD void finalizeTrial(const StabilityResidual<NC> &s, const double *ref, Trial<NC> &t) const
     {
         double dist = 0.0;
 #pragma unroll
@@ -1346,7 +1345,7 @@ struct Solver
     }
 
     // stabilityTrial_ (stability.inc:225-355)
-    __device__ __noinline__ void stabilityTrial(int candidate, double P, double T, const double *logRef,
+    NZ_HDN void stabilityTrial(int candidate, double P, double T, const double *logRef,
                                                 const double *ref, const double *seedIn, Trial<NC> &t)
     {
         t.valid = false;
@@ -1361,7 +1360,7 @@ struct Solver
 #pragma unroll
         for (int i = 0; i < NC; ++i)
             logW[i] = log(smax(seed[i], O().floor));
-        const int ssiSteps = min(O().maxStability, max(O().stabilitySsi, 0));
+        const int ssiSteps = imin(O().maxStability, imax(O().stabilitySsi, 0));
         StabilityResidual<NC> cur, probe;
 #pragma unroll 1
         for (int it = 0; it < ssiSteps; ++it)
@@ -1435,7 +1434,7 @@ struct Solver
             if (!accepted)
                 break;
         }
-        const int remaining = max(0, O().maxStability - ssiSteps);
+        const int remaining = imax(0, O().maxStability - ssiSteps);
 #pragma unroll 1
         for (int it = 0; it < remaining; ++it)
         {
@@ -1454,9 +1453,9 @@ struct Solver
     }
 
     // stabilitySeeds_ (stability.inc:32-96): seed k of the candidate list.
-    __device__ int stabilitySeedCount() const { return NC + 6 + ((F->water >= 0 && NC > 1) ? 1 : 0); }
+    NZ_HD int stabilitySeedCount() const { return NC + 6 + ((F->water >= 0 && NC > 1) ? 1 : 0); }
 
-    __device__ void stabilitySeed(int k, double P, double T, const double *z, const double *ref, double *seed)
+    NZ_HD void stabilitySeed(int k, double P, double T, const double *z, const double *ref, double *seed)
     {
         if (k < 4)
         {
@@ -1500,7 +1499,7 @@ struct Solver
     }
 
     // stabilityTest (three_phase_flash.hpp:300-489)
-    __device__ __noinline__ void stabilityTest(double P, double T, const double *zIn, uint8_t active,
+    NZ_HDN void stabilityTest(double P, double T, const double *zIn, uint8_t active,
                                                const double (&activeX)[3][NC], StabilityResult<NC> &res)
     {
         res.stable = true;
@@ -1604,7 +1603,7 @@ struct Solver
             Trial<NC> best, trial;
             best.valid = false;
             best.trivial = false;
-            best.sum = -__longlong_as_double(0x7ff0000000000000LL);
+            best.sum = -nzInf();
             const int nseeds = stabilitySeedCount();
 #pragma unroll 1
             for (int k = 0; k < nseeds; ++k)
@@ -1650,7 +1649,7 @@ struct Solver
 
     // --------------------------------------------------- canonicalisation --
     // refreshCanonicalThermodynamics_ (canonicalization.inc:47-66)
-    __device__ void refreshCanonical(double P, double T, Result<NC> &r)
+    NZ_HD void refreshCanonical(double P, double T, Result<NC> &r)
     {
         double phi[NC];
         for (int p = 0; p < 3; ++p)
@@ -1665,7 +1664,7 @@ struct Solver
     }
 
     // canonicalizeLiquidRoles_ (canonicalization.inc:99-135)
-    __device__ void canonicalizeLiquidRoles(Result<NC> &r) const
+    NZ_HD void canonicalizeLiquidRoles(Result<NC> &r) const
     {
         if (F->water < 0)
             return;
@@ -1687,7 +1686,7 @@ struct Solver
     }
 
     // canonicalize_ (canonicalization.inc:8-45)
-    __device__ __noinline__ void canonicalize(double P, double T, Result<NC> &r)
+    NZ_HDN void canonicalize(double P, double T, Result<NC> &r)
     {
         uint8_t p = presenceFromFractions(r.beta);
         if (p == 0)
@@ -1725,7 +1724,7 @@ struct Solver
     }
 
     // canonicalizeGlobalWaterRole_ (canonicalization.inc:175-224)
-    __device__ int canonicalizeGlobalWaterRole(Result<NC> &r) const
+    NZ_HD int canonicalizeGlobalWaterRole(Result<NC> &r) const
     {
         if (F->water < 0)
             return -1;
@@ -1760,7 +1759,7 @@ struct Solver
     }
 
     // validatePhysicalFlashResult_ (canonicalization.inc:225-321)
-    __device__ __noinline__ bool validatePhysical(double P, double T, const double *z, const Result<NC> &r)
+    NZ_HDN bool validatePhysical(double P, double T, const double *z, const Result<NC> &r)
     {
         if (!r.converged)
             return false;
@@ -1826,7 +1825,7 @@ struct Solver
     }
 
     // overallComposition_ (canonicalization.inc:323-337)
-    __device__ void overallComposition(const Result<NC> &r, double *z)
+    NZ_HD void overallComposition(const Result<NC> &r, double *z)
     {
 #pragma unroll
         for (int i = 0; i < NC; ++i)
@@ -1844,7 +1843,7 @@ struct Solver
     }
 
     // reequilibrateCanonicalRoles_ (canonicalization.inc:339-377)
-    __device__ void reequilibrateCanonicalRoles(double P, double T, const double *z, Result<NC> &seed,
+    NZ_HD void reequilibrateCanonicalRoles(double P, double T, const double *z, Result<NC> &seed,
                                                 Result<NC> &out)
     {
         seed.presence = presenceFromFractions(seed.beta);
@@ -1876,7 +1875,7 @@ struct Solver
     }
 
     // canonicalizeNonAqueousRoles_ (canonicalization.inc:379-414)
-    __device__ bool canonicalizeNonAqueousRoles(double P, double T, Result<NC> &r) const
+    NZ_HD bool canonicalizeNonAqueousRoles(double P, double T, Result<NC> &r) const
     {
         const bool hasOil = r.beta[0] > O().betaTol;
         const bool hasGas = r.beta[1] > O().betaTol;
@@ -1900,7 +1899,7 @@ struct Solver
     }
 
     // expectedSingleNonAqueousRole_ (canonicalization.inc:416-439)
-    __device__ int expectedSingleNonAqueousRole(double P, double T, const double *x) const
+    NZ_HD int expectedSingleNonAqueousRole(double P, double T, const double *x) const
     {
         double wilson[NC];
         wilsonK(P, T, wilson);
@@ -1916,7 +1915,7 @@ struct Solver
     }
 
     // canonicalizeSingleNonAqueousRole_ (canonicalization.inc:441-463)
-    __device__ bool canonicalizeSingleNonAqueousRole(double P, double T, Result<NC> &r) const
+    NZ_HD bool canonicalizeSingleNonAqueousRole(double P, double T, Result<NC> &r) const
     {
         const bool hasOil = r.beta[0] > O().betaTol;
         const bool hasGas = r.beta[1] > O().betaTol;
@@ -1932,7 +1931,7 @@ struct Solver
     }
 
     // canonicalizeCoalescedSwSingleNonAqueousRole_ (canonicalization.inc:466-498)
-    __device__ void canonicalizeCoalescedSwSingle(double P, double T, Result<NC> &r)
+    NZ_HD void canonicalizeCoalescedSwSingle(double P, double T, Result<NC> &r)
     {
         if (!sw())
             return;
@@ -1951,7 +1950,7 @@ struct Solver
     }
 
     // collapseCoincidentSwPhases_ (canonicalization.inc:507-586)
-    __device__ void collapseCoincidentSw(double P, double T, Result<NC> &r)
+    NZ_HD void collapseCoincidentSw(double P, double T, Result<NC> &r)
     {
         if (!sw() || !(O().coincidentTol > 0.0))
             return;
@@ -2008,7 +2007,7 @@ struct Solver
     }
 
     // swThermodynamicRolesConsistent_ (canonicalization.inc:588-686)
-    __device__ bool swRolesConsistent(double P, double T, const Result<NC> &r, bool preserveRestricted)
+    NZ_HD bool swRolesConsistent(double P, double T, const Result<NC> &r, bool preserveRestricted)
     {
         if (!sw() || F->water < 0)
             return true;
@@ -2075,7 +2074,7 @@ struct Solver
     }
 
     // canonicalizeSwThermodynamicRoles_ (canonicalization.inc:688-712)
-    __device__ void canonicalizeSwRoles(Result<NC> &r) const
+    NZ_HD void canonicalizeSwRoles(Result<NC> &r) const
     {
         Result<NC> c = r;
         for (int p = 0; p < 3; ++p)
@@ -2105,7 +2104,7 @@ struct Solver
     }
 
     // canonicalizeFinal_ (canonicalization.inc:714-796)
-    __device__ __noinline__ void canonicalizeFinal(double P, double T, Result<NC> &r, bool preserveRestricted)
+    NZ_HDN void canonicalizeFinal(double P, double T, Result<NC> &r, bool preserveRestricted)
     {
         if (!r.converged)
             return;
@@ -2153,9 +2152,556 @@ struct Solver
         r.converged = false;
     }
 
+
+    // ------------------------------------------- SW allocation recovery ----
+    // evaluateAllocation_ (allocation.inc:31-128): softmax allocation u -> state
+    struct AllocState
+    {
+        bool valid;
+        double gibbs;
+        double closure;
+        double residualNorm2;
+        double residual[2 * NC];
+        double gradient[2 * NC];
+        double x[3][NC];
+        double beta[3];
+        double Z[3];
+    };
+
+    NZ_HDN void evaluateAllocation(double P, double T, const double *z, const double *u, AllocState &s)
+    {
+        s.valid = false;
+        s.gibbs = 0.0;
+        s.closure = nzInf();
+        s.residualNorm2 = nzInf();
+        s.beta[0] = s.beta[1] = s.beta[2] = 0.0;
+        double amount[3][NC];
+#pragma unroll 1
+        for (int c = 0; c < NC; ++c)
+        {
+            const double ug = u[c];
+            const double uw = u[NC + c];
+            const double shift = smax3(0.0, ug, uw);
+            const double qo0 = exp(-shift);
+            const double qg0 = exp(ug - shift);
+            const double qw0 = exp(uw - shift);
+            const double qsum = qo0 + qg0 + qw0;
+            const double qo = qo0 / qsum, qg = qg0 / qsum, qw = qw0 / qsum;
+            amount[0][c] = z[c] * qo;
+            amount[1][c] = z[c] * qg;
+            amount[2][c] = z[c] * qw;
+            s.beta[0] += amount[0][c];
+            s.beta[1] += amount[1][c];
+            s.beta[2] += amount[2][c];
+        }
+        for (int p = 0; p < 3; ++p)
+        {
+            if (!(s.beta[p] > 1.0e-14))
+                return;
+#pragma unroll 1
+            for (int c = 0; c < NC; ++c)
+                s.x[p][c] = amount[p][c] / s.beta[p];
+        }
+        double mu[3][NC];
+        double phi[NC];
+        for (int p = 0; p < 3; ++p)
+        {
+            s.Z[p] = phase(p, P, T, s.x[p], phi);
+#pragma unroll 1
+            for (int c = 0; c < NC; ++c)
+            {
+                const double xv = smax(s.x[p][c], O().floor);
+                const double ph = smax(phi[c], 1.0e-300);
+                mu[p][c] = log(xv) + log(ph);
+                s.gibbs += amount[p][c] * mu[p][c];
+            }
+        }
+        s.closure = 0.0;
+        s.residualNorm2 = 0.0;
+#pragma unroll 1
+        for (int c = 0; c < NC; ++c)
+        {
+            const int w = NC + c;
+            if (!(z[c] > O().floor))
+            {
+                s.residual[c] = s.residual[w] = 0.0;
+                s.gradient[c] = s.gradient[w] = 0.0;
+                continue;
+            }
+            s.residual[c] = mu[1][c] - mu[0][c];
+            s.residual[w] = mu[2][c] - mu[0][c];
+            s.residualNorm2 += s.residual[c] * s.residual[c] + s.residual[w] * s.residual[w];
+            double cl = s.closure;
+            const double d01 = fabs(mu[0][c] - mu[1][c]);
+            const double d02 = fabs(mu[0][c] - mu[2][c]);
+            const double d12 = fabs(mu[1][c] - mu[2][c]);
+            if (cl < d01) cl = d01;
+            if (cl < d02) cl = d02;
+            if (cl < d12) cl = d12;
+            s.closure = cl;
+            const double qo = amount[0][c] / z[c];
+            const double qg = amount[1][c] / z[c];
+            const double qw = amount[2][c] / z[c];
+            const double average = qo * mu[0][c] + qg * mu[1][c] + qw * mu[2][c];
+            s.gradient[c] = z[c] * qg * (mu[1][c] - average);
+            s.gradient[w] = z[c] * qw * (mu[2][c] - average);
+        }
+        s.valid = isfinite(s.gibbs) && isfinite(s.residualNorm2) && isfinite(s.closure);
+    }
+
+    // gibbsPreconditionAllocation_ (allocation.inc:134-239): BFGS on the Gibbs energy
+    NZ_HDN void gibbsPrecondition(double P, double T, const double *z, double *u, AllocState &state)
+    {
+        constexpr int M = 2 * NC;
+        double H[M][M];
+        for (int i = 0; i < M; ++i)
+            for (int j = 0; j < M; ++j)
+                H[i][j] = i == j ? 1.0 : 0.0;
+        evaluateAllocation(P, T, z, u, state);
+        if (!state.valid)
+            return;
+        AllocState trial;
+#pragma unroll 1
+        for (int it = 0; it < 160; ++it)
+        {
+            if (err)
+                return;
+            double dir[M];
+            for (int i = 0; i < M; ++i)
+            {
+                dir[i] = 0.0;
+                for (int j = 0; j < M; ++j)
+                    dir[i] -= H[i][j] * state.gradient[j];
+            }
+            double dd = 0.0, maxStep = 0.0;
+            for (int i = 0; i < M; ++i)
+            {
+                dd += state.gradient[i] * dir[i];
+                maxStep = smax(maxStep, fabs(dir[i]));
+            }
+            if (!(dd < 0.0) || !isfinite(dd))
+            {
+                dd = 0.0;
+                maxStep = 0.0;
+                for (int i = 0; i < M; ++i)
+                {
+                    for (int j = 0; j < M; ++j)
+                        H[i][j] = i == j ? 1.0 : 0.0;
+                    dir[i] = -state.gradient[i];
+                    dd += state.gradient[i] * dir[i];
+                    maxStep = smax(maxStep, fabs(dir[i]));
+                }
+            }
+            if (maxStep > 4.0)
+                for (int i = 0; i < M; ++i)
+                    dir[i] *= 4.0 / maxStep;
+            double trialU[M];
+            double step = 1.0;
+            bool accepted = false;
+#pragma unroll 1
+            for (int ls = 0; ls < 24; ++ls)
+            {
+                for (int i = 0; i < M; ++i)
+                    trialU[i] = sclamp(u[i] + step * dir[i], -40.0, 40.0);
+                evaluateAllocation(P, T, z, trialU, trial);
+                if (trial.valid && trial.gibbs <= state.gibbs + 1.0e-4 * step * dd)
+                {
+                    accepted = true;
+                    break;
+                }
+                step *= 0.5;
+            }
+            if (!accepted)
+                return;
+            double sv[M], yv[M], hy[M];
+            double ys = 0.0;
+            for (int i = 0; i < M; ++i)
+            {
+                sv[i] = trialU[i] - u[i];
+                yv[i] = trial.gradient[i] - state.gradient[i];
+            }
+            for (int i = 0; i < M; ++i)
+                ys += yv[i] * sv[i];
+            if (ys > 1.0e-12)
+            {
+                for (int i = 0; i < M; ++i)
+                {
+                    hy[i] = 0.0;
+                    for (int j = 0; j < M; ++j)
+                        hy[i] += H[i][j] * yv[j];
+                }
+                double yhy = 0.0;
+                for (int i = 0; i < M; ++i)
+                    yhy += yv[i] * hy[i];
+                const double coef = (ys + yhy) / (ys * ys);
+                for (int i = 0; i < M; ++i)
+                    for (int j = 0; j < M; ++j)
+                        H[i][j] += coef * sv[i] * sv[j] - (hy[i] * sv[j] + sv[i] * hy[j]) / ys;
+            }
+            else
+            {
+                for (int i = 0; i < M; ++i)
+                    for (int j = 0; j < M; ++j)
+                        H[i][j] = i == j ? 1.0 : 0.0;
+            }
+            for (int i = 0; i < M; ++i)
+                u[i] = trialU[i];
+            state = trial;
+        }
+    }
+
+    // refineAllocationChemicalPotentials_ (allocation.inc:246-346): LM on mu differences
+    NZ_HDN bool refineAllocation(double P, double T, const double *z, double *u, AllocState &state)
+    {
+        constexpr int M = 2 * NC;
+        evaluateAllocation(P, T, z, u, state);
+        if (!state.valid)
+            return false;
+        double lambda = 1.0e-5;
+        AllocState ps, ms, trial;
+        double J[M][M];
+#pragma unroll 1
+        for (int it = 0; it < 160; ++it)
+        {
+            if (err)
+                return false;
+            if (state.closure < O().fugacityTol)
+                return true;
+#pragma unroll 1
+            for (int col = 0; col < M; ++col)
+            {
+                const double h = 2.0e-5 * smax(1.0, fabs(u[col]));
+                double plus[M], minus[M];
+                for (int i = 0; i < M; ++i)
+                    plus[i] = minus[i] = u[i];
+                plus[col] = smin(40.0, u[col] + h);
+                minus[col] = smax(-40.0, u[col] - h);
+                evaluateAllocation(P, T, z, plus, ps);
+                evaluateAllocation(P, T, z, minus, ms);
+                if (!ps.valid || !ms.valid)
+                    return false;
+                const double den = plus[col] - minus[col];
+                for (int row = 0; row < M; ++row)
+                    J[row][col] = (ps.residual[row] - ms.residual[row]) / den;
+            }
+            bool accepted = false;
+#pragma unroll 1
+            for (int lm = 0; lm < 14 && !accepted; ++lm)
+            {
+                double Nm[M][M], rhs[M], delta[M];
+                for (int a = 0; a < M; ++a)
+                {
+                    for (int b = 0; b < M; ++b)
+                    {
+                        double v = 0.0;
+                        for (int row = 0; row < M; ++row)
+                            v += J[row][a] * J[row][b];
+                        Nm[a][b] = v;
+                    }
+                    double v = 0.0;
+                    for (int row = 0; row < M; ++row)
+                        v += J[row][a] * state.residual[row];
+                    rhs[a] = -v;
+                    Nm[a][a] += lambda;
+                }
+                if (!solveDense<M>(Nm, rhs, delta))
+                {
+                    lambda *= 10.0;
+                    continue;
+                }
+                double maxDelta = 0.0;
+                for (int i = 0; i < M; ++i)
+                    maxDelta = smax(maxDelta, fabs(delta[i]));
+                if (maxDelta > 6.0)
+                    for (int i = 0; i < M; ++i)
+                        delta[i] *= 6.0 / maxDelta;
+                double damping = 1.0;
+#pragma unroll 1
+                for (int ls = 0; ls < 22; ++ls)
+                {
+                    double trialU[M];
+                    for (int i = 0; i < M; ++i)
+                        trialU[i] = sclamp(u[i] + damping * delta[i], -40.0, 40.0);
+                    evaluateAllocation(P, T, z, trialU, trial);
+                    if (trial.valid && trial.residualNorm2 < state.residualNorm2 * (1.0 - 1.0e-5 * damping))
+                    {
+                        for (int i = 0; i < M; ++i)
+                            u[i] = trialU[i];
+                        state = trial;
+                        lambda = smax(1.0e-14, lambda * 0.2);
+                        accepted = true;
+                        break;
+                    }
+                    damping *= 0.5;
+                }
+                if (!accepted)
+                    lambda *= 10.0;
+            }
+            if (!accepted)
+                return false;
+        }
+        return state.closure < O().fugacityTol;
+    }
+
+    // amounts -> allocation variables (shared tail of the seed builders)
+    NZ_HD void allocationFromAmounts(const double *z, const double (&amount)[3][NC], double *u) const
+    {
+        for (int c = 0; c < NC; ++c)
+        {
+            if (!(z[c] > O().floor))
+            {
+                u[c] = 0.0;
+                u[NC + c] = 0.0;
+                continue;
+            }
+            const double qo = smax(amount[0][c] / z[c], 1.0e-18);
+            const double qg = smax(amount[1][c] / z[c], 1.0e-18);
+            const double qw = smax(amount[2][c] / z[c], 1.0e-18);
+            u[c] = log(qg / qo);
+            u[NC + c] = log(qw / qo);
+        }
+    }
+
+    // allocationSeedFromPair_ (allocation.inc:361-446)
+    NZ_HDN bool allocationSeedFromPair(double P, double T, const double *z, uint8_t allowed, double *u)
+    {
+        Result<NC> pair;
+        flashRestrictedRecovery(P, T, z, allowed, pair);
+        if (!pair.converged || popcount3(pair.presence) != 2)
+            return false;
+        StabilityResult<NC> st;
+        stabilityTest(P, T, z, pair.presence, pair.x, st);
+        int missing = -1;
+        for (int p = 0; p < 3; ++p)
+            if (!(pair.presence & bitOf(p)))
+            {
+                missing = p;
+                break;
+            }
+        if (missing < 0 || !st.valid || !st.unstable[missing])
+            return false;
+        const double *inc = st.incipient[missing];
+        double eps = 1.0e-3;
+        for (int c = 0; c < NC; ++c)
+            if (inc[c] > 1.0e-30)
+                eps = smin(eps, 0.15 * z[c] / inc[c]);
+        eps = smax(eps, 1.0e-9);
+        double amount[3][NC];
+        for (int p = 0; p < 3; ++p)
+            for (int c = 0; c < NC; ++c)
+                amount[p][c] = 0.0;
+        for (int c = 0; c < NC; ++c)
+        {
+            if (!(z[c] > O().floor))
+                continue;
+            amount[missing][c] = eps * inc[c];
+            const double remaining = z[c] - amount[missing][c];
+            if (!(remaining > 0.0))
+                return false;
+            double pairAmount = 0.0;
+            for (int p = 0; p < 3; ++p)
+                if (p != missing)
+                    pairAmount += pair.beta[p] * pair.x[p][c];
+            if (!(pairAmount > 0.0))
+                return false;
+            for (int p = 0; p < 3; ++p)
+                if (p != missing)
+                    amount[p][c] = pair.beta[p] * pair.x[p][c] * remaining / pairAmount;
+        }
+        allocationFromAmounts(z, amount, u);
+        return true;
+    }
+
+    // allocationSeedFromRawOg_ (allocation.inc:449-502)
+    NZ_HDN bool allocationSeedFromRawOg(double P, double T, const double *z, double *u)
+    {
+        double kg[NC];
+        wilsonK(P, T, kg);
+        Result<NC> pair;
+        flashTwo(P, T, z, OIL, GAS, kg, pair);
+        if (!pair.converged || popcount3(presenceFromFractions(pair.beta)) != 2)
+            return false;
+        pair.presence = presenceFromFractions(pair.beta);
+        StabilityResult<NC> st;
+        stabilityTest(P, T, z, pair.presence, pair.x, st);
+        if (!st.valid || !st.unstable[WATER])
+            return false;
+        const double *inc = st.incipient[WATER];
+        double eps = 1.0e-3;
+        for (int c = 0; c < NC; ++c)
+            if (inc[c] > 1.0e-30)
+                eps = smin(eps, 0.2 * z[c] / inc[c]);
+        eps = smax(eps, 1.0e-9);
+        double amount[3][NC];
+        for (int c = 0; c < NC; ++c)
+        {
+            if (!(z[c] > O().floor))
+            {
+                u[c] = 0.0;
+                u[NC + c] = 0.0;
+                continue;
+            }
+            amount[2][c] = eps * inc[c];
+            const double remaining = z[c] - amount[2][c];
+            const double no = pair.beta[0] * pair.x[0][c];
+            const double ng = pair.beta[1] * pair.x[1][c];
+            const double sum = no + ng;
+            if (!(remaining > 0.0) || !(sum > 0.0))
+                return false;
+            amount[0][c] = no * remaining / sum;
+            amount[1][c] = ng * remaining / sum;
+            const double qo = smax(amount[0][c] / z[c], 1.0e-18);
+            const double qg = smax(amount[1][c] / z[c], 1.0e-18);
+            const double qw = smax(amount[2][c] / z[c], 1.0e-18);
+            u[c] = log(qg / qo);
+            u[NC + c] = log(qw / qo);
+        }
+        return true;
+    }
+
+    // allocationSeedFromSingle_ (allocation.inc:504-578)
+    NZ_HDN bool allocationSeedFromSingle(double P, double T, const double *z, double *u)
+    {
+        const uint8_t active = chooseSinglePhase(P, T, z);
+        Result<NC> single;
+        singlePhaseResult(P, T, z, active, single);
+        StabilityResult<NC> st;
+        stabilityTest(P, T, z, active, single.x, st);
+        if (!st.valid || st.stable)
+            return false;
+        double eps[3] = {0.0, 0.0, 0.0};
+        int missingCount = 0;
+        for (int p = 0; p < 3; ++p)
+            if (!(active & bitOf(p)) && st.unstable[p])
+            {
+                eps[p] = 1.0e-4;
+                ++missingCount;
+            }
+        if (missingCount == 0)
+            return false;
+        for (int c = 0; c < NC; ++c)
+            for (int p = 0; p < 3; ++p)
+            {
+                if (!(eps[p] > 0.0))
+                    continue;
+                eps[p] = smin(eps[p], 0.08 * z[c] / smax(st.incipient[p][c], 1.0e-30));
+            }
+        double amount[3][NC];
+        for (int p = 0; p < 3; ++p)
+            for (int c = 0; c < NC; ++c)
+                amount[p][c] = 0.0;
+        const int activeSlot = firstActive(active);
+        for (int c = 0; c < NC; ++c)
+        {
+            if (!(z[c] > O().floor))
+            {
+                u[c] = 0.0;
+                u[NC + c] = 0.0;
+                continue;
+            }
+            double removed = 0.0;
+            for (int p = 0; p < 3; ++p)
+            {
+                if (!(eps[p] > 0.0))
+                    continue;
+                amount[p][c] = eps[p] * st.incipient[p][c];
+                removed += amount[p][c];
+            }
+            if (!(z[c] > removed))
+                return false;
+            amount[activeSlot][c] = z[c] - removed;
+            const double qo = smax(amount[0][c] / z[c], 1.0e-18);
+            const double qg = smax(amount[1][c] / z[c], 1.0e-18);
+            const double qw = smax(amount[2][c] / z[c], 1.0e-18);
+            u[c] = log(qg / qo);
+            u[NC + c] = log(qw / qo);
+        }
+        return true;
+    }
+
+    // thermodynamicAllocationSeed_ (allocation.inc:581-604)
+    NZ_HD void thermodynamicAllocationSeed(double P, double T, double scale, double gs, double ws, double *u) const
+    {
+        double kg[NC], kw[NC];
+        wilsonK(P, T, kg);
+        initialWaterK(kw);
+        for (int c = 0; c < NC; ++c)
+        {
+            u[c] = sclamp(scale * log(sclamp(kg[c], 1.0e-30, 1.0e30)) + gs, -30.0, 30.0);
+            u[NC + c] = sclamp(scale * log(sclamp(kw[c], 1.0e-30, 1.0e30)) + ws, -30.0, 30.0);
+        }
+    }
+
+    // flashThreeAllocationFallback_ (allocation.inc:609-700).  The 23 seeds
+    // are built and processed in the reference's order; seed construction is
+    // independent of the processing, so it is done lazily per seed.
+    NZ_HDN void allocationFallback(double P, double T, const double *z, Result<NC> &best)
+    {
+        best.init();
+        double bestG = nzInf();
+        const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
+        const double thermo[6][3] = {{1.0, 0.0, 0.0}, {0.5, 0.0, 0.0}, {1.5, 0.0, 0.0},
+                                     {1.0, -1.5, -1.5}, {1.0, 1.5, -1.5}, {1.0, -1.5, 1.5}};
+        const double generic[12][2] = {{0.0, 0.0}, {1.0, -2.0}, {2.0, -4.0}, {2.0, -2.0},
+                                       {1.0, -4.0}, {-1.0, -1.0}, {-2.0, -2.0}, {-2.0, 1.0},
+                                       {-1.0, 2.0}, {2.0, 1.0}, {1.0, 2.0}, {-2.0, 2.0}};
+        AllocState state;
+        Result<NC> cand;
+#pragma unroll 1
+        for (int k = 0; k < 23; ++k)
+        {
+            if (err)
+                return;
+            double u[2 * NC];
+            bool valid = true;
+            if (k == 0)
+                valid = allocationSeedFromRawOg(P, T, z, u);
+            else if (k == 1)
+                valid = allocationSeedFromSingle(P, T, z, u);
+            else if (k < 5)
+                valid = allocationSeedFromPair(P, T, z, pairs[k - 2], u);
+            else if (k < 11)
+                thermodynamicAllocationSeed(P, T, thermo[k - 5][0], thermo[k - 5][1], thermo[k - 5][2], u);
+            else
+                for (int c = 0; c < NC; ++c)
+                {
+                    u[c] = generic[k - 11][0];
+                    u[NC + c] = generic[k - 11][1];
+                }
+            if (!valid)
+                continue;
+            gibbsPrecondition(P, T, z, u, state);
+            if (!state.valid)
+                continue;
+            if (!refineAllocation(P, T, z, u, state))
+                continue;
+            if (!(state.beta[0] > O().betaTol) || !(state.beta[1] > O().betaTol) ||
+                !(state.beta[2] > O().betaTol))
+                continue;
+            if (!(state.gibbs < bestG))
+                continue;
+            cand.init();
+            cand.converged = true;
+            cand.presence = ALL_BITS;
+            for (int p = 0; p < 3; ++p)
+            {
+                cand.beta[p] = state.beta[p];
+                cand.Z[p] = state.Z[p];
+                for (int c = 0; c < NC; ++c)
+                    cand.x[p][c] = state.x[p][c];
+            }
+            deriveReferenceK(cand);
+            updateSaturations(P, T, cand);
+            if (!cand.converged)
+                continue;
+            best = cand;
+            bestG = state.gibbs;
+        }
+    }
+
     // ------------------------------------------------------- active set ----
     // equilibrateActiveSet_ (allocation.inc:707-858)
-    __device__ __noinline__ void equilibrateActiveSet(double P, double T, const double *z, uint8_t active,
+    NZ_HDN void equilibrateActiveSet(double P, double T, const double *z, uint8_t active,
                                                       Result<NC> &seed, bool reuseConvergedSeed,
                                                       Result<NC> &out)
     {
@@ -2286,7 +2832,7 @@ struct Solver
     // ------------------------------------------------- restricted flashes --
     // flashRestrictedImpl_ (restricted.inc:8-59).  A three-phase `allowed`
     // set is never requested by the entry points carried here.
-    __device__ __noinline__ void flashRestrictedImpl(double P, double T, const double *zIn, uint8_t allowed,
+    NZ_HDN void flashRestrictedImpl(double P, double T, const double *zIn, uint8_t allowed,
                                                      const double (*seedX)[3][NC], Result<NC> &r)
     {
         r.init();
@@ -2342,7 +2888,7 @@ struct Solver
     }
 
     // flashRestricted (three_phase_flash.hpp:235-292), both overloads
-    __device__ __noinline__ void flashRestricted(double P, double T, const double *zIn, uint8_t allowed,
+    NZ_HDN void flashRestricted(double P, double T, const double *zIn, uint8_t allowed,
                                                  const double (*seedX)[3][NC], Result<NC> &r)
     {
         double z[NC];
@@ -2366,7 +2912,7 @@ struct Solver
     }
 
     // flashRestrictedRecovery_ (restricted.inc:629-646)
-    __device__ void flashRestrictedRecovery(double P, double T, const double *zIn, uint8_t allowed, Result<NC> &r)
+    NZ_HD void flashRestrictedRecovery(double P, double T, const double *zIn, uint8_t allowed, Result<NC> &r)
     {
         double z[NC];
 #pragma unroll
@@ -2383,10 +2929,10 @@ struct Solver
     }
 
     // stableReducedSetFallback_ (restricted.inc:655-693)
-    __device__ __noinline__ void stableReducedSetFallback(double P, double T, const double *z, Result<NC> &best)
+    NZ_HDN void stableReducedSetFallback(double P, double T, const double *z, Result<NC> &best)
     {
         best.init();
-        double bestG = __longlong_as_double(0x7ff0000000000000LL);
+        double bestG = nzInf();
         const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
         Result<NC> cand;
         for (int k = 0; k < 3; ++k)
@@ -2413,7 +2959,7 @@ struct Solver
     }
 
     // preferStableSwReducedOverSingle_ (restricted.inc:703-780)
-    __device__ __noinline__ void preferStableSwReducedOverSingle(double P, double T, const double *z,
+    NZ_HDN void preferStableSwReducedOverSingle(double P, double T, const double *z,
                                                                  Result<NC> &cand)
     {
         if (!sw() || popcount3(presenceFromFractions(cand.beta)) != 1)
@@ -2424,7 +2970,7 @@ struct Solver
         const bool singleKnownUnstable = single.valid && !single.stable;
         Result<NC> reduced, trial;
         reduced.init();
-        double reducedG = __longlong_as_double(0x7ff0000000000000LL);
+        double reducedG = nzInf();
         const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
         for (int k = 0; k < 3; ++k)
         {
@@ -2465,7 +3011,7 @@ struct Solver
     }
 
     // numericalSwRoleResult_ (restricted.inc:514-541)
-    __device__ void numericalSwRoleResult(const Result<NC> &c, Result<NC> &n) const
+    NZ_HD void numericalSwRoleResult(const Result<NC> &c, Result<NC> &n) const
     {
         n = c;
         if (!sw())
@@ -2500,7 +3046,7 @@ struct Solver
     // role-permutation search and the pressure continuation run with both
     // recoveries disabled, exactly like the reference (core.inc:47-57).
     template <bool TopLevel>
-    __device__ __noinline__ void flash(double P, double T, const double *zIn, Result<NC> &out)
+    NZ_HDN void flash(double P, double T, const double *zIn, Result<NC> &out)
     {
         out.init();
         if (!validatePT(P, T))
@@ -2586,9 +3132,70 @@ struct Solver
             return;
         if (sw())
         {
-            // recovery 3 (SW only): exact-mass allocation basin search -- not carried.
-            fail(ERR_NOT_PORTED);
-            return;
+            // recovery 3 (SW only): exact-mass allocation basin search
+            Result<NC> allocated;
+            allocationFallback(P, T, z, allocated);
+            if (err)
+                return;
+            if (allocated.converged)
+            {
+                canonicalizeFinal(P, T, allocated, false);
+                if (allocated.converged && validatePhysical(P, T, z, allocated))
+                {
+                    preferStableSwReducedOverSingle(P, T, z, allocated);
+                    if (allocated.converged)
+                    {
+                        out = allocated;
+                        return;
+                    }
+                }
+            }
+        }
+        if (TopLevel && sw() && permutationSearch)
+        {
+            // recovery 4 (SW only): the other fixed role permutations (three_phase_flash.hpp:174-205)
+            Result<NC> bestPermuted, permuted;
+            bestPermuted.init();
+            double bestG = nzInf();
+#pragma unroll 1
+            for (int k = 0; k < 6; ++k)
+            {
+                int perm[3];
+                swRolePermutation(k, perm);
+                if (perm[0] == roles[0] && perm[1] == roles[1] && perm[2] == roles[2])
+                    continue;
+                Solver<NC> cand = *this;
+                cand.roles[0] = perm[0];
+                cand.roles[1] = perm[1];
+                cand.roles[2] = perm[2];
+                cand.permutationSearch = false;
+                cand.continuation = false;
+                cand.template flash<false>(P, T, z, permuted);
+                const bool ok = permuted.converged && cand.err == ERR_NONE;
+                const double g = ok ? cand.dimensionlessGibbs(P, T, permuted) : 0.0;
+                evals = cand.evals;
+                if (cand.err)
+                {
+                    fail(cand.err);
+                    return;
+                }
+                if (!ok)
+                    continue;
+                if (isfinite(g) && g < bestG)
+                {
+                    bestG = g;
+                    bestPermuted = permuted;
+                }
+            }
+            if (bestPermuted.converged)
+            {
+                preferStableSwReducedOverSingle(P, T, z, bestPermuted);
+                if (bestPermuted.converged)
+                {
+                    out = bestPermuted;
+                    return;
+                }
+            }
         }
         if (TopLevel && continuation)
         {
@@ -2611,7 +3218,7 @@ struct Solver
     }
 
     // pressureContinuationFallback_ (restricted.inc:554-627)
-    __device__ __noinline__ void pressureContinuation(double P, double T, const double *z, Result<NC> &out)
+    NZ_HDN void pressureContinuation(double P, double T, const double *z, Result<NC> &out)
     {
         out.init();
         if (!(P > 0.0))
