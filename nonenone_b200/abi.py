@@ -19,6 +19,7 @@ FLASH_CONVERGED, FLASH_FAILED, FLASH_BAD_INPUT, FLASH_EOS_ERROR, FLASH_NOT_PORTE
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_FP64_STAGED = 2
 
 OIL, GAS, WATER = 0, 1, 2
 

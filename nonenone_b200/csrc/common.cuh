@@ -11,6 +11,8 @@ namespace nz
 {
 
 constexpr int kFlashBlock = 128;
+constexpr int kTrialBlock = 128;
+constexpr int kTrialBlocksPerSm = 8;
 
 int setError(int code, const char *fmt, ...);
 int cudaFail(cudaError_t e, const char *what);
@@ -28,6 +30,12 @@ struct nz_ctx
     nz::FluidDev fluid{};
     unsigned long long *evalCounter{nullptr};   // EOS evaluations of the last flash batch
     cudaStream_t ownStream{nullptr};
+    int smCount{148};
+    void *scratch{nullptr};                     // staged-flash work space (grow only)
+    size_t scratchBytes{0};
+
+    // Make the work space at least `bytes` large (cudaMalloc on growth only).
+    int ensureScratch(size_t bytes);
 
     cudaStream_t hostStream()
     {
@@ -39,8 +47,9 @@ struct nz_ctx
 
 namespace nz
 {
-int launchMixedFlash(nz_ctx *ctx, int64_t n, const double *P, const double *T, const double *z,
-                     const double *sal, const nz_flash_out &out, cudaStream_t st);
+template <int NC>
+int launchStaged(nz_ctx *ctx, int64_t n, const double *P, const double *T, const double *z,
+                 const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st);
 }
 
 // Runtime nc -> compile-time NC dispatch over the instantiated component counts.

@@ -21,7 +21,9 @@
 #define NZ_HD __device__
 #define NZ_HDI __device__ __forceinline__
 #define NZ_HDN __device__ __noinline__
+#define NZ_BOTH __host__ __device__ inline
 #else
+#define NZ_BOTH inline
 #include <cmath>
 #include <cstring>
 using std::isfinite;

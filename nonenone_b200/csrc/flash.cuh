@@ -37,7 +37,7 @@ struct Result
     double Kg[NC];
     double Kw[NC];
 
-    NZ_HD void init()
+    NZ_HDN void init()
     {
         converged = false;
         iterations = 0;
@@ -210,6 +210,10 @@ struct Solver
     bool continuation;
     int err;
     unsigned long long evals;
+    // Warp-cooperative mode: all `width` lanes run the same point in lockstep
+    // and split the seeds of every stability test (width 1 = one thread).
+    int lane;
+    int width;
     // cubic parameter cache (core.inc:71-99)
     bool cacheValid;
     double cacheP, cacheT;
@@ -225,6 +229,8 @@ struct Solver
         continuation = true;
         err = ERR_NONE;
         evals = 0;
+        lane = 0;
+        width = 1;
         cacheValid = false;
         cacheP = cacheT = 0.0;
     }
@@ -366,7 +372,7 @@ struct Solver
     }
 
     // solveRr3_ (nonlinear.inc:8-96)
-    NZ_HD bool rr3(const double *z, const double *kg, const double *kw, double initBg, double initBw,
+    NZ_HDN bool rr3(const double *z, const double *kg, const double *kw, double initBg, double initBw,
                         double &outBg, double &outBw) const
     {
         double bg = sclamp(initBg, 1.0e-4, 0.8);
@@ -420,7 +426,7 @@ struct Solver
     }
 
     // solveRr3Robust_ (nonlinear.inc:98-127)
-    NZ_HD bool rr3Robust(const double *z, const double *kg, const double *kw, double pg, double pw,
+    NZ_HDN bool rr3Robust(const double *z, const double *kg, const double *kw, double pg, double pw,
                               double &bg, double &bw) const
     {
         const double guesses[17][2] = {
@@ -453,7 +459,7 @@ struct Solver
         return f;
     }
 
-    NZ_HD bool rr2(const double *z, const double *K, double initialBeta, double &out) const
+    NZ_HDN bool rr2(const double *z, const double *K, double initialBeta, double &out) const
     {
         double d0;
         const double f0 = rr2Eval(z, K, 0.0, d0);
@@ -510,7 +516,7 @@ struct Solver
 
     // updateSaturationsFromMoles (three_phase_flash.hpp:527-575).  No aqueous
     // volume closure is configured, so every Water composition is admissible.
-    NZ_HD void updateSaturations(double P, double T, Result<NC> &r)
+    NZ_HDN void updateSaturations(double P, double T, Result<NC> &r)
     {
         double volumeSum = 0.0;
         double volume[3] = {0.0, 0.0, 0.0};
@@ -544,7 +550,7 @@ struct Solver
     }
 
     // singlePhaseResult_ (restricted.inc:425-447)
-    NZ_HD void singlePhaseResult(double P, double T, const double *z, uint8_t active, Result<NC> &r)
+    NZ_HDN void singlePhaseResult(double P, double T, const double *z, uint8_t active, Result<NC> &r)
     {
         r.init();
         r.converged = true;
@@ -580,7 +586,7 @@ struct Solver
     }
 
     // chooseSinglePhase_ (restricted.inc:449-478)
-    NZ_HD uint8_t chooseSinglePhase(double P, double T, const double *z)
+    NZ_HDN uint8_t chooseSinglePhase(double P, double T, const double *z)
     {
         double phi[NC];
         double g[3];
@@ -607,7 +613,7 @@ struct Solver
     }
 
     // dimensionlessGibbs_ (restricted.inc:480-505); the public slot is the role.
-    NZ_HD double dimensionlessGibbs(double P, double T, const Result<NC> &r)
+    NZ_HDN double dimensionlessGibbs(double P, double T, const Result<NC> &r)
     {
         double g = 0.0;
         double phi[NC];
@@ -646,7 +652,7 @@ struct Solver
 
     // ------------------------------------------------------- pair seeds ----
     // pairInitialK_ (nonlinear.inc:515-623)
-    NZ_HD void pairInitialK(int first, int second, double P, double T, const double *z, double *K)
+    NZ_HDN void pairInitialK(int first, int second, double P, double T, const double *z, double *K)
     {
         if (sw() && (first == WATER || second == WATER))
         {
@@ -781,7 +787,7 @@ struct Solver
     }
 
     // one damped SSI step of flashTwo_ (restricted.inc:155-208)
-    NZ_HD bool twoSsiStep(double P, double T, const double *z, int first, int second, double *K,
+    NZ_HDN bool twoSsiStep(double P, double T, const double *z, int first, int second, double *K,
                                double &betaSecond, int &totalIterations, Result<NC> &r)
     {
         double bS;
@@ -957,7 +963,7 @@ struct Solver
     }
 
     // finalizePhysicallyConvergedTwoPhase_ (restricted.inc:336-412)
-    NZ_HD void finalizePhysicallyConvergedTwoPhase(double P, double T, const double *z, int first,
+    NZ_HDN void finalizePhysicallyConvergedTwoPhase(double P, double T, const double *z, int first,
                                                         int second, Result<NC> &r)
     {
         if (r.converged)
@@ -1083,7 +1089,7 @@ struct Solver
     }
 
     // one damped SSI step of flashThree_ (nonlinear.inc:301-371)
-    NZ_HD bool threeSsiStep(double P, double T, const double *z, double *kg, double *kw,
+    NZ_HDN bool threeSsiStep(double P, double T, const double *z, double *kg, double *kw,
                                  double &bg, double &bw, int &total, Result<NC> &r)
     {
         double ng, nw;
@@ -1287,7 +1293,7 @@ struct Solver
 
     // ----------------------------------------------------- stability -------
     // evaluateStabilityResidual_ (stability.inc:157-204)
-    NZ_HD void stabilityResidual(int candidate, double P, double T, const double *logRef,
+    NZ_HDN void stabilityResidual(int candidate, double P, double T, const double *logRef,
                                       const double *logW, StabilityResidual<NC> &s)
     {
         s.valid = false;
@@ -1455,7 +1461,7 @@ struct Solver
     // stabilitySeeds_ (stability.inc:32-96): seed k of the candidate list.
     NZ_HD int stabilitySeedCount() const { return NC + 6 + ((F->water >= 0 && NC > 1) ? 1 : 0); }
 
-    NZ_HD void stabilitySeed(int k, double P, double T, const double *z, const double *ref, double *seed)
+    NZ_HDN void stabilitySeed(int k, double P, double T, const double *z, const double *ref, double *seed)
     {
         if (k < 4)
         {
@@ -1496,6 +1502,47 @@ struct Solver
         for (int i = 0; i < NC; ++i)
             seed[i] = trace;
         seed[F->water] = 1.0 - 1.0e-6;
+    }
+
+    // Lanes hold the first-best trial of their own seeds (seed k on lane
+    // k % width); the warp's answer is the largest trial sum, ties going to
+    // the lowest seed index -- the sequential loop's first-best rule.  The
+    // error flag is shared too, since one failing trial aborts the flash.
+    NZ_HD void warpCombineTrials(Trial<NC> &best, int bestK)
+    {
+#ifdef __CUDA_ARCH__
+        __syncwarp();
+        int e = err;
+        for (int off = 16; off > 0; off >>= 1)
+            e = imax(e, __shfl_xor_sync(0xffffffffu, e, off));
+        err = e;
+        double key = best.valid ? best.sum : -nzInf();
+        int kk = best.valid ? bestK : 0x7fffffff;
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            const double ok = __shfl_xor_sync(0xffffffffu, key, off);
+            const int ik = __shfl_xor_sync(0xffffffffu, kk, off);
+            if (ok > key || (ok == key && ik < kk))
+            {
+                key = ok;
+                kk = ik;
+            }
+        }
+        if (kk == 0x7fffffff)
+        {
+            best.valid = false;
+            return;
+        }
+        const int src = kk % width;
+        best.valid = true;
+        best.trivial = __shfl_sync(0xffffffffu, int(best.trivial), src) != 0;
+        best.sum = __shfl_sync(0xffffffffu, best.sum, src);
+        for (int i = 0; i < NC; ++i)
+            best.x[i] = __shfl_sync(0xffffffffu, best.x[i], src);
+#else
+        (void)best;
+        (void)bestK;
+#endif
     }
 
     // stabilityTest (three_phase_flash.hpp:300-489)
@@ -1605,17 +1652,25 @@ struct Solver
             best.trivial = false;
             best.sum = -nzInf();
             const int nseeds = stabilitySeedCount();
+            int bestK = -1;
 #pragma unroll 1
-            for (int k = 0; k < nseeds; ++k)
+            for (int k = lane; k < nseeds; k += width)
             {
                 double seed[NC];
                 stabilitySeed(k, P, T, z, refX, seed);
                 stabilityTrial(cand, P, T, logRef, refX, seed, trial);
                 if (trial.valid && (!best.valid || trial.sum > best.sum))
+                {
                     best = trial;
-                if (err)
+                    bestK = k;
+                }
+                if (err && width == 1)
                     return;
             }
+            if (width > 1)
+                warpCombineTrials(best, bestK);
+            if (err)
+                return;
             if (!best.valid)
             {
                 res.valid = false;
@@ -1649,7 +1704,7 @@ struct Solver
 
     // --------------------------------------------------- canonicalisation --
     // refreshCanonicalThermodynamics_ (canonicalization.inc:47-66)
-    NZ_HD void refreshCanonical(double P, double T, Result<NC> &r)
+    NZ_HDN void refreshCanonical(double P, double T, Result<NC> &r)
     {
         double phi[NC];
         for (int p = 0; p < 3; ++p)
@@ -1664,7 +1719,7 @@ struct Solver
     }
 
     // canonicalizeLiquidRoles_ (canonicalization.inc:99-135)
-    NZ_HD void canonicalizeLiquidRoles(Result<NC> &r) const
+    NZ_HDN void canonicalizeLiquidRoles(Result<NC> &r) const
     {
         if (F->water < 0)
             return;
@@ -1724,7 +1779,7 @@ struct Solver
     }
 
     // canonicalizeGlobalWaterRole_ (canonicalization.inc:175-224)
-    NZ_HD int canonicalizeGlobalWaterRole(Result<NC> &r) const
+    NZ_HDN int canonicalizeGlobalWaterRole(Result<NC> &r) const
     {
         if (F->water < 0)
             return -1;
@@ -1825,7 +1880,7 @@ struct Solver
     }
 
     // overallComposition_ (canonicalization.inc:323-337)
-    NZ_HD void overallComposition(const Result<NC> &r, double *z)
+    NZ_HDN void overallComposition(const Result<NC> &r, double *z)
     {
 #pragma unroll
         for (int i = 0; i < NC; ++i)
@@ -1843,7 +1898,7 @@ struct Solver
     }
 
     // reequilibrateCanonicalRoles_ (canonicalization.inc:339-377)
-    NZ_HD void reequilibrateCanonicalRoles(double P, double T, const double *z, Result<NC> &seed,
+    NZ_HDN void reequilibrateCanonicalRoles(double P, double T, const double *z, Result<NC> &seed,
                                                 Result<NC> &out)
     {
         seed.presence = presenceFromFractions(seed.beta);
@@ -1875,7 +1930,7 @@ struct Solver
     }
 
     // canonicalizeNonAqueousRoles_ (canonicalization.inc:379-414)
-    NZ_HD bool canonicalizeNonAqueousRoles(double P, double T, Result<NC> &r) const
+    NZ_HDN bool canonicalizeNonAqueousRoles(double P, double T, Result<NC> &r) const
     {
         const bool hasOil = r.beta[0] > O().betaTol;
         const bool hasGas = r.beta[1] > O().betaTol;
@@ -1899,7 +1954,7 @@ struct Solver
     }
 
     // expectedSingleNonAqueousRole_ (canonicalization.inc:416-439)
-    NZ_HD int expectedSingleNonAqueousRole(double P, double T, const double *x) const
+    NZ_HDN int expectedSingleNonAqueousRole(double P, double T, const double *x) const
     {
         double wilson[NC];
         wilsonK(P, T, wilson);
@@ -1915,7 +1970,7 @@ struct Solver
     }
 
     // canonicalizeSingleNonAqueousRole_ (canonicalization.inc:441-463)
-    NZ_HD bool canonicalizeSingleNonAqueousRole(double P, double T, Result<NC> &r) const
+    NZ_HDN bool canonicalizeSingleNonAqueousRole(double P, double T, Result<NC> &r) const
     {
         const bool hasOil = r.beta[0] > O().betaTol;
         const bool hasGas = r.beta[1] > O().betaTol;
@@ -1931,7 +1986,7 @@ struct Solver
     }
 
     // canonicalizeCoalescedSwSingleNonAqueousRole_ (canonicalization.inc:466-498)
-    NZ_HD void canonicalizeCoalescedSwSingle(double P, double T, Result<NC> &r)
+    NZ_HDN void canonicalizeCoalescedSwSingle(double P, double T, Result<NC> &r)
     {
         if (!sw())
             return;
@@ -1950,7 +2005,7 @@ struct Solver
     }
 
     // collapseCoincidentSwPhases_ (canonicalization.inc:507-586)
-    NZ_HD void collapseCoincidentSw(double P, double T, Result<NC> &r)
+    NZ_HDN void collapseCoincidentSw(double P, double T, Result<NC> &r)
     {
         if (!sw() || !(O().coincidentTol > 0.0))
             return;
@@ -2007,7 +2062,7 @@ struct Solver
     }
 
     // swThermodynamicRolesConsistent_ (canonicalization.inc:588-686)
-    NZ_HD bool swRolesConsistent(double P, double T, const Result<NC> &r, bool preserveRestricted)
+    NZ_HDN bool swRolesConsistent(double P, double T, const Result<NC> &r, bool preserveRestricted)
     {
         if (!sw() || F->water < 0)
             return true;
@@ -2074,7 +2129,7 @@ struct Solver
     }
 
     // canonicalizeSwThermodynamicRoles_ (canonicalization.inc:688-712)
-    NZ_HD void canonicalizeSwRoles(Result<NC> &r) const
+    NZ_HDN void canonicalizeSwRoles(Result<NC> &r) const
     {
         Result<NC> c = r;
         for (int p = 0; p < 3; ++p)
@@ -2912,7 +2967,7 @@ struct Solver
     }
 
     // flashRestrictedRecovery_ (restricted.inc:629-646)
-    NZ_HD void flashRestrictedRecovery(double P, double T, const double *zIn, uint8_t allowed, Result<NC> &r)
+    NZ_HDN void flashRestrictedRecovery(double P, double T, const double *zIn, uint8_t allowed, Result<NC> &r)
     {
         double z[NC];
 #pragma unroll
@@ -3011,7 +3066,7 @@ struct Solver
     }
 
     // numericalSwRoleResult_ (restricted.inc:514-541)
-    NZ_HD void numericalSwRoleResult(const Result<NC> &c, Result<NC> &n) const
+    NZ_HDN void numericalSwRoleResult(const Result<NC> &c, Result<NC> &n) const
     {
         n = c;
         if (!sw())

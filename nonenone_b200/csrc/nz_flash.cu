@@ -144,6 +144,7 @@ int nz_ctx_create(const nz_fluid_desc *fluid, const nz_flash_options *options, i
     c->desc = *fluid;
     c->options = opts;
     c->fluid = makeFluidDev(*fluid, opts);
+    cudaDeviceGetAttribute(&c->smCount, cudaDevAttrMultiProcessorCount, device);
     e = cudaMalloc(&c->evalCounter, sizeof(unsigned long long));
     if (e != cudaSuccess)
     {
@@ -162,6 +163,10 @@ int nz_ctx_destroy(nz_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->evalCounter)
         cudaFree(ctx->evalCounter);
+    if (ctx->scratch)
+        cudaFree(ctx->scratch);
+    if (ctx->ownStream)
+        cudaStreamDestroy(ctx->ownStream);
     delete ctx;
     return NZ_OK;
 }
@@ -196,7 +201,8 @@ int nz_flash_batch(nz_ctx *ctx, int64_t n, const double *P, const double *T, con
 {
     if (!ctx || !out || n < 0 || (n > 0 && (!P || !T || !z)))
         return setError(NZ_ERR_ARGUMENT, "nz_flash_batch: bad argument");
-    if (precision != NZ_PRECISION_FP64 && precision != NZ_PRECISION_MIXED)
+    if (precision != NZ_PRECISION_FP64 && precision != NZ_PRECISION_MIXED &&
+        precision != NZ_PRECISION_FP64_STAGED)
         return setError(NZ_ERR_ARGUMENT, "nz_flash_batch: unknown precision %d", precision);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(ctx->evalCounter, 0, sizeof(unsigned long long), st);
@@ -204,15 +210,14 @@ int nz_flash_batch(nz_ctx *ctx, int64_t n, const double *P, const double *T, con
         return cudaFail(e, "nz_flash_batch counter reset");
     if (n == 0)
         return NZ_OK;
-    if (precision == NZ_PRECISION_MIXED)
+    if (precision == NZ_PRECISION_FP64)
     {
-        const int rc = launchMixedFlash(ctx, n, P, T, z, salinity, *out, st);
-        if (rc != NZ_OK)
-            return rc;
+        DISPATCH_NC(ctx->fluid.nc, launchFlash, ctx, n, P, T, z, salinity, *out, st);
     }
     else
     {
-        DISPATCH_NC(ctx->fluid.nc, launchFlash, ctx, n, P, T, z, salinity, *out, st);
+        const bool mixed = precision == NZ_PRECISION_MIXED;
+        DISPATCH_NC(ctx->fluid.nc, launchStaged, ctx, n, P, T, z, salinity, *out, mixed, st);
     }
     e = cudaGetLastError();
     return e == cudaSuccess ? NZ_OK : cudaFail(e, "nz_flash_batch launch");
@@ -300,13 +305,19 @@ int nz_flash_batch_host(nz_ctx *ctx, int64_t n, const double *P, const double *T
 
 } // extern "C"
 
-namespace nz
+int nz_ctx::ensureScratch(size_t bytes)
 {
-// The mixed-precision batched form lives in nz_mixed.cu once built; until
-// then the entry point refuses the precision instead of silently running FP64.
-__attribute__((weak)) int launchMixedFlash(nz_ctx *, int64_t, const double *, const double *, const double *,
-                                           const double *, const nz_flash_out &, cudaStream_t)
-{
-    return setError(NZ_ERR_UNSUPPORTED, "nz_flash_batch: NZ_PRECISION_MIXED is not built");
+    if (bytes <= scratchBytes)
+        return NZ_OK;
+    if (scratch)
+    {
+        cudaFree(scratch);
+        scratch = nullptr;
+        scratchBytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&scratch, bytes);
+    if (e != cudaSuccess)
+        return nz::cudaFail(e, "staged flash work space");
+    scratchBytes = bytes;
+    return NZ_OK;
 }
-} // namespace nz

@@ -184,3 +184,30 @@ def test_stability_matches_reference(torch_cuda, reference, golden):
     miss = np.stack([((g["presence"][idx] >> p) & 1) == 0 for p in range(3)])
     err = np.abs(s["trial_sum"] - r["trial_sum"])[miss]
     assert err.max() < 1e-7
+
+
+@pytest.mark.parametrize("name,fluid_args", [
+    ("flash_pr_nc3.npz", dict()),
+    ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
+    ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
+])
+def test_staged_fp64_matches_golden(torch_cuda, golden, name, fluid_args):
+    """The staged FP64 form (driver / trial kernels) against the reference."""
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    g = golden(name)
+    fl = CubicThreePhaseFlash(make_fluid(**fluid_args))
+    out = _np(fl.flash(g["P"], g["T"], g["z"], salinity=g.get("salinity"),
+                       precision=abi.PRECISION_FP64_STAGED))
+    compare_flash(out, g)
+
+
+def test_staged_fp64_equals_plain_fp64(torch_cuda, golden):
+    """Staging changes the schedule, not the arithmetic: same labels, values to rounding."""
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    g = golden("flash_pr_nc3.npz")
+    fl = CubicThreePhaseFlash(make_fluid())
+    a = _np(fl.flash(g["P"], g["T"], g["z"], precision=abi.PRECISION_FP64))
+    b = _np(fl.flash(g["P"], g["T"], g["z"], precision=abi.PRECISION_FP64_STAGED))
+    assert np.array_equal(a["status"], b["status"]) and np.array_equal(a["presence"], b["presence"])
+    ok = a["status"] == 0
+    assert np.abs(a["beta"][:, ok] - b["beta"][:, ok]).max() < 1e-13
