@@ -170,6 +170,31 @@ int nz_flash_batch_host(nz_ctx* ctx, int64_t n, const double* pressure,
  * nz_flash_batch on this context executed; read after a stream sync. */
 int nz_flash_eos_eval_count(nz_ctx* ctx, uint64_t* count);
 
+/* ---- P-T-z flash without allocation ------------------------------------------
+ * No counterpart in the reference (it has no GPU code): an extra entry point
+ * for callers that must not allocate device memory while they run -- hosts
+ * whose device memory is pre-claimed by another allocator (a PETSc or
+ * framework memory pool holding the GPU, so a cudaMalloc at call time can
+ * fail or fragment their pool) and deployments that fix every device
+ * allocation at load time.  It runs the staged batched flash
+ * (NZ_PRECISION_FP64_STAGED or NZ_PRECISION_MIXED) with its work space in a
+ * static device array of NZ_NOALLOC_SCRATCH_BYTES that every GPU which loads
+ * this library holds until the process exits; it calls no cudaMalloc /
+ * cudaFree.  Batches whose work space would exceed the array are rejected
+ * with NZ_ERR_ARGUMENT (at most 14,846 points for nc = 3, 8,120 for nc = 6,
+ * 5,970 for nc = 8).  The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress) and
+ * should therefore come before any stream capture.  All calls share the one
+ * array and the context's evaluation counter: calls that overlap on the GPU
+ * (other streams, other contexts) race and must be serialised by the caller.
+ * Device pointers, stream ordered, same outputs as nz_flash_batch.
+ */
+#define NZ_NOALLOC_SCRATCH_BYTES (32ull << 20)
+int nz_flash_batch_noalloc(nz_ctx* ctx, int64_t n, const double* pressure,
+                           const double* temperature, const double* z,
+                           const double* salinity, const nz_flash_out* out,
+                           int32_t precision, void* stream);
+
 /* ---- tangent-plane stability ----------------------------------------------
  * Replaces CubicThreePhaseFlash::stabilityTest (three_phase_flash.hpp:300-489)
  * for a batch.  active[n] PhasePresence bits of the tested set,

@@ -11,6 +11,9 @@ MAX_NC = 8
 
 NZ_OK = 0
 NZ_RECOVERABLE = 1
+NZ_ERR_ARGUMENT = -1
+NZ_ERR_CUDA = -2
+NZ_ERR_UNSUPPORTED = -3
 
 EOS_PR, EOS_SW, EOS_CPA = 0, 1, 2
 SW_BIP_KIJ, SW_BIP_CONSTANT, SW_BIP_CO2, SW_BIP_HYDROCARBON, SW_BIP_CO2_CHABAB = range(5)

@@ -50,6 +50,15 @@ namespace nz
 template <int NC>
 int launchStaged(nz_ctx *ctx, int64_t n, const double *P, const double *T, const double *z,
                  const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st);
+// The staged flash into a caller-provided work space of `capacity` bytes.
+template <int NC>
+int launchStagedInto(nz_ctx *ctx, void *scratch, size_t capacity, int64_t n, const double *P, const double *T,
+                     const double *z, const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st);
+// Work-space bytes of an n-point staged flash, and the largest n that fits.
+size_t stagedScratchBytesFor(int nc, int64_t n, const FluidDev &F);
+int64_t stagedMaxPointsFor(int nc, size_t capacity, const FluidDev &F);
+template <int NC>
+size_t stagedScratchBytesNc(int64_t n, const FluidDev &F);
 }
 
 // Runtime nc -> compile-time NC dispatch over the instantiated component counts.

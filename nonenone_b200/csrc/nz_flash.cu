@@ -305,6 +305,38 @@ int nz_flash_batch_host(nz_ctx *ctx, int64_t n, const double *P, const double *T
 
 } // extern "C"
 
+namespace nz
+{
+size_t stagedScratchBytesFor(int nc, int64_t n, const FluidDev &F)
+{
+    switch (nc)
+    {
+    case 3: return stagedScratchBytesNc<3>(n, F);
+    case 4: return stagedScratchBytesNc<4>(n, F);
+    case 5: return stagedScratchBytesNc<5>(n, F);
+    case 6: return stagedScratchBytesNc<6>(n, F);
+    case 8: return stagedScratchBytesNc<8>(n, F);
+    default: return ~size_t(0);
+    }
+}
+
+int64_t stagedMaxPointsFor(int nc, size_t capacity, const FluidDev &F)
+{
+    int64_t lo = 0, hi = 1;
+    while (stagedScratchBytesFor(nc, hi, F) <= capacity && hi < (int64_t(1) << 40))
+        hi *= 2;
+    while (hi - lo > 1)
+    {
+        const int64_t mid = (lo + hi) / 2;
+        if (stagedScratchBytesFor(nc, mid, F) <= capacity)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+} // namespace nz
+
 int nz_ctx::ensureScratch(size_t bytes)
 {
     if (bytes <= scratchBytes)

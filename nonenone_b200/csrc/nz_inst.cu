@@ -28,6 +28,24 @@ int launchStaged(nz_ctx *ctx, int64_t n, const double *P, const double *T, const
         return rc;
     return stagedLaunch<NC>(ctx->fluid, ctx->scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st);
 }
+template <int NC>
+int launchStagedInto(nz_ctx *ctx, void *scratch, size_t capacity, int64_t n, const double *P, const double *T,
+                     const double *z, const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st)
+{
+    (void)mixed;
+    if (stagedScratchBytes<NC>(n, ctx->fluid) > capacity)
+        return setError(NZ_ERR_ARGUMENT, "staged flash: work space too small");
+    return stagedLaunch<NC>(ctx->fluid, scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st);
+}
+template <int NC>
+size_t stagedScratchBytesNc(int64_t n, const FluidDev &F)
+{
+    return stagedScratchBytes<NC>(n, F);
+}
+template int launchStagedInto<NZ_INST_NC>(nz_ctx *, void *, size_t, int64_t, const double *, const double *,
+                                          const double *, const double *, const nz_flash_out &, bool,
+                                          cudaStream_t);
+template size_t stagedScratchBytesNc<NZ_INST_NC>(int64_t, const FluidDev &);
 template int launchStaged<NZ_INST_NC>(nz_ctx *, int64_t, const double *, const double *, const double *,
                                       const double *, const nz_flash_out &, bool, cudaStream_t);
 } // namespace nz

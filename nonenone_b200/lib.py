@@ -19,6 +19,7 @@ EXPORTED = (
     "nz_flash_eos_eval_count", "nz_stability_batch", "nz_natural_create",
     "nz_natural_destroy", "nz_natural_pattern", "nz_natural_set_history",
     "nz_update_state", "nz_residual", "nz_jacobian", "nz_diag_fma_peak",
+    "nz_flash_batch_noalloc",
 )
 
 _lib = None
@@ -57,6 +58,7 @@ def load():
         L.nz_residual.argtypes = [vp, vp, vp, vp, vp]
         L.nz_jacobian.argtypes = [vp, vp, vp, vp, vp, vp]
     L.nz_diag_fma_peak.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.nz_flash_batch_noalloc.argtypes = [vp, i64, vp, vp, vp, vp, vp, i32, vp]
     if L.nz_abi_version() != 1:
         raise NzError("ABI version mismatch")
     _lib = L
