@@ -22,6 +22,8 @@
  *                        (natural_petsc_runtime_residual.inc:19-133)
  *   nz_jacobian          NaturalPetscRuntime::assembleJacobian_
  *                        (natural_petsc_runtime_jacobian.inc:8-109,120-299)
+ *   nz_natural_init_ptz  NaturalPetscRuntime::initializeUniformFromPTZ
+ *                        (natural_petsc_runtime_state.inc:107-164), per cell
  *   nz_natural_pattern   buildNaturalJacobianPattern
  *                        (models/include/natural/petsc/jacobian_factory.hpp:39-245)
  */
@@ -261,6 +263,16 @@ int nz_natural_destroy(nz_natural* nat);
  * (columns sorted, self included).  nnzb via *nnzb when col_idx is NULL. */
 int nz_natural_pattern(nz_natural* nat, int64_t* row_ptr, int64_t* col_idx,
                        int64_t* nnzb);
+/* Per-cell P-T-z initialisation: flashPTZ + assignFlashResult into a default
+ * phase state, as NaturalPetscRuntime::initializeUniformFromPTZ
+ * (natural_petsc_runtime_state.inc:107-164) does for one uniform (P, z), here
+ * with one (P, z) per cell.  P[ncell], z[ncell][nc] (cell-major), primary and
+ * phase_state outputs, all device pointers.  Returns NZ_RECOVERABLE, with
+ * *first_failure = the lowest failing cell, when a flash does not converge
+ * (the reference throws); nothing is written then. */
+int nz_natural_init_ptz(nz_natural* nat, const double* P, const double* z,
+                        double* primary, double* phase_state,
+                        int64_t* first_failure, void* stream);
 /* Accepted history: previous-time accumulation M^n from primary/phase state
  * (refreshPreviousPropertiesCache_, natural_petsc_runtime_cache_history.inc:180-262). */
 int nz_natural_set_history(nz_natural* nat, const double* primary,

@@ -1,0 +1,52 @@
+// nat_inst.cu -- Natural kernels of one component count (NZ_INST_NC).
+#include "natural_host.cuh"
+#include "natural_kernels.cuh"
+
+#ifndef NZ_INST_NC
+#error "NZ_INST_NC must be defined"
+#endif
+
+namespace nz
+{
+template <int NC>
+int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
+{
+    const int64_t n = a.g.ncell;
+    const unsigned grid = unsigned((n + kNatBlock - 1) / kNatBlock);
+    switch (op)
+    {
+    case NAT_CACHE:
+        natCacheKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.flag);
+        break;
+    case NAT_RESIDUAL:
+        natResidualKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.residual, a.flag);
+        break;
+    case NAT_JACOBIAN:
+    {
+        constexpr int perWarp = 32 / Layout<NC>::B;
+        const int64_t warps = (n + perWarp - 1) / perWarp;
+        const unsigned jgrid = unsigned((warps * 32 + kNatBlock - 1) / kNatBlock);
+        natJacobianKernel<NC><<<jgrid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.values, a.residual,
+                                                          a.flag);
+        break;
+    }
+    case NAT_HISTORY:
+        natHistoryKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.prevAcc, a.flag);
+        break;
+    case NAT_UPDATE:
+        natUpdateKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, n, a.primary, a.ps, a.newPrimary, a.newPs,
+                                                       a.status, a.firstFailure);
+        break;
+    case NAT_INIT:
+        natInitKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
+                                                     a.firstFailure);
+        break;
+    default:
+        return setError(NZ_ERR_ARGUMENT, "natLaunch: unknown operation %d", op);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? NZ_OK : cudaFail(e, "Natural kernel launch");
+}
+
+template int natLaunch<NZ_INST_NC>(int, const NatLaunch &, cudaStream_t);
+} // namespace nz

@@ -19,7 +19,7 @@ EXPORTED = (
     "nz_flash_eos_eval_count", "nz_stability_batch", "nz_natural_create",
     "nz_natural_destroy", "nz_natural_pattern", "nz_natural_set_history",
     "nz_update_state", "nz_residual", "nz_jacobian", "nz_diag_fma_peak",
-    "nz_flash_batch_noalloc",
+    "nz_flash_batch_noalloc", "nz_natural_init_ptz",
 )
 
 _lib = None
@@ -53,6 +53,7 @@ def load():
         L.nz_natural_create.argtypes = [vp, vp, C.POINTER(vp)]
         L.nz_natural_destroy.argtypes = [vp]
         L.nz_natural_pattern.argtypes = [vp, vp, vp, vp]
+        L.nz_natural_init_ptz.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.nz_natural_set_history.argtypes = [vp, vp, vp, vp]
         L.nz_update_state.argtypes = [vp, vp, vp, vp, vp]
         L.nz_residual.argtypes = [vp, vp, vp, vp, vp]

@@ -59,3 +59,55 @@ def raw_box_points(n: int, seed: int = 12345):
     T = rng.uniform(303.0, 423.0, n)
     z = np.ascontiguousarray(rng.dirichlet([2.0, 1.0, 1.0], n).T)
     return P, T, z
+
+
+def natural_case(seed: int = 0, nx: int = 60, ny: int = 20, nz: int = 1,
+                 dx: float = 10.0, dy: float = 10.0, dz: float = 5.0,
+                 perm_median_md: float = 100.0, perm_sigma_ln: float = 1.0,
+                 kv_kh: float = 1.0, porosity=(0.15, 0.25), pressure=(10e6, 30e6),
+                 alpha=(2.0, 1.0, 1.0)):
+    """One Newton evaluation's inputs on a structured grid.
+
+    Defaults are the 60x20x1 H2O/CO2/nC10 case: 10 m x 10 m x 5 m cells,
+    permeability lognormal (median 100 mD, sigma_ln 1), porosity U[0.15, 0.25],
+    P ~ U[10, 30] MPa, z ~ Dirichlet(2, 1, 1).  Returns (grid, P[ncell],
+    z[ncell, nc]).
+    """
+    from .grid import MILLIDARCY, StructuredGrid
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    kh = perm_median_md * MILLIDARCY * np.exp(perm_sigma_ln * rng.standard_normal(n))
+    perm = np.stack([kh, kh, kh * kv_kh], axis=1)
+    phi = rng.uniform(porosity[0], porosity[1], n)
+    grid = StructuredGrid(nx, ny, nz, dx, dy, dz, perm, phi)
+    P = rng.uniform(pressure[0], pressure[1], n)
+    z = rng.dirichlet(list(alpha), n)
+    return grid, P, np.ascontiguousarray(z)
+
+
+# Quadratic relative permeabilities of the reference's H2O-CO2-nC10 case
+# (case/h2o_co2_nc10_2d_benchmark/benchmark_common.hpp:97-126).
+RELPERM_H2O_CO2_NC10 = dict(swc=0.10, sorw=0.15, sgc=0.02, sorg=0.10,
+                            krw_max=0.30, krg_max=0.80, kro_max=0.80)
+
+
+def perturb_natural_state(primary, phase_state, nc: int, seed: int, scale: float = 1.0,
+                          remove_fraction: float = 0.1):
+    """A Newton iterate near an accepted Natural state (cell-major numpy arrays):
+    pressure, phase compositions and saturations jittered, and on
+    ``remove_fraction`` of the cells one present phase pushed to a saturation
+    of 5e-5 (below the 1e-4 active-set boundary) so that it is removed."""
+    rng = np.random.default_rng(seed)
+    p = np.array(primary, dtype=np.float64, copy=True)
+    n = p.shape[0]
+    p[:, 0] *= 1.0 + 0.02 * scale * rng.standard_normal(n)
+    ncomp = 3 * (nc - 1)
+    p[:, 1:1 + ncomp] += 0.01 * scale * rng.standard_normal((n, ncomp))
+    p[:, 1 + ncomp:] += 0.05 * scale * rng.standard_normal((n, 3))
+    flags = np.rint(np.asarray(phase_state)[:, 0]).astype(np.int64)
+    pick = np.where(rng.uniform(size=n) < remove_fraction)[0]
+    for c in pick:
+        present = [ph for ph in range(3) if (flags[c] >> ph) & 1]
+        ph = present[rng.integers(len(present))]
+        p[c, 1 + ncomp + ph] = 5.0e-5
+    return p

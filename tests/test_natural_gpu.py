@@ -1,0 +1,193 @@
+"""GPU Natural assembly parity: P-T-z initialisation, residual, BAIJ Jacobian
+and the transactional phase-state update, through the C ABI, against the
+reference's own FP64 code (golden fixtures, and the live oracle at full size).
+
+Tolerances:
+  * Jacobian pattern (row_ptr / col_idx) and phase labels: bit-exact;
+  * residual and Jacobian entries: |gpu - ref| <= 1e-9 * max(|ref|, 1e-6 * s_e),
+    with s_e the largest |ref| of that equation row over all cells (so entries
+    that are rounding noise next to their row's terms are compared absolutely);
+  * primaries and phase-state values: 1e-8 relative (scale max(1, |ref|)).
+"""
+import types
+
+import numpy as np
+import pytest
+
+from nonenone_b200 import abi, synth
+from nonenone_b200.fluids import SIX_COMPONENT, make_fluid
+
+pytestmark = pytest.mark.gpu
+
+ENTRY_TOL = 1e-9
+FLOOR = 1e-6
+STATE_TOL = 1e-8
+REPORT_FIELDS = [f for f, _ in abi.Report._fields_]
+
+CASES = {
+    "natural_pr_nc3.npz": lambda: make_fluid(),
+    "natural_sw_nc3.npz": lambda: make_fluid(eos_model=abi.EOS_SW, salinity=1.0),
+    "natural_pr_nc6.npz": lambda: make_fluid(SIX_COMPONENT),
+}
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a visible CUDA device")
+    return torch
+
+
+def grid_of(g):
+    return types.SimpleNamespace(
+        ncell=g["porosity"].shape[0], porosity=g["porosity"], volume=g["volume"],
+        conn_offset=g["conn_offset"], conn_neighbor=g["conn_neighbor"],
+        conn_trans=g["conn_trans"], conn_gravity=g["conn_gravity"])
+
+
+def assembler(fluid, grid, time_step=864.0, temperature=353.15):
+    from nonenone_b200.flash import Context
+    from nonenone_b200.natural import NaturalAssembler
+    ctx = Context(fluid)
+    nat = NaturalAssembler(ctx, grid, time_step, temperature,
+                           abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10))
+    nat._ctx_keep = ctx
+    return nat
+
+
+def assert_entries(gpu, ref, axis_eq, what):
+    """Entry-wise check with the per-equation-row floor described above."""
+    gpu = np.asarray(gpu)
+    ref = np.asarray(ref)
+    assert np.array_equal(np.isnan(gpu), np.isnan(ref)), f"{what}: NaN pattern differs"
+    fin = ~np.isnan(ref)
+    red = tuple(a for a in range(ref.ndim) if a != axis_eq)
+    scale = np.nanmax(np.abs(ref), axis=red, keepdims=True)
+    denom = np.maximum(np.abs(ref), FLOOR * scale)
+    err = np.where(fin, np.abs(gpu - ref) / np.where(denom > 0, denom, 1.0), 0.0)
+    worst = np.unravel_index(np.argmax(err), err.shape)
+    assert err.max() <= ENTRY_TOL, f"{what}: max err {err.max():.3e} at {worst}: {gpu[worst]} vs {ref[worst]}"
+    return err.max()
+
+
+def assert_state(gpu_p, gpu_s, ref_p, ref_s, what):
+    assert np.array_equal(gpu_s[:, 0], ref_s[:, 0]), (
+        f"{what}: phase labels differ at cells {np.where(gpu_s[:, 0] != ref_s[:, 0])[0][:10]}")
+    assert np.array_equal(gpu_s[:, -1], ref_s[:, -1]), f"{what}: suppression flags differ"
+    for name, a, b in (("primary", gpu_p, ref_p), ("phase_state", gpu_s, ref_s)):
+        err = np.abs(a - b) / np.maximum(1.0, np.abs(b))
+        assert err.max() <= STATE_TOL, (what, name, err.max(), np.unravel_index(err.argmax(), err.shape))
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request, golden, torch_cuda):
+    g = golden(request.param)
+    fluid = CASES[request.param]()
+    nat = assembler(fluid, grid_of(g), float(g["time_step"]), float(g["temperature"]))
+    return request.param, g, nat
+
+
+def test_pattern_matches_reference(case):
+    _, g, nat = case
+    rp, ci = nat.pattern()
+    assert np.array_equal(rp, g["row_ptr"]) and np.array_equal(ci, g["col_idx"])
+
+
+def test_initialize_from_ptz(case):
+    name, g, nat = case
+    primary, ps = nat.initialize_from_ptz(g["P"], g["z"])
+    assert_state(primary.cpu().numpy(), ps.cpu().numpy(), g["primary"], g["phase_state"], name)
+
+
+def test_residual_and_jacobian(case, torch_cuda):
+    torch = torch_cuda
+    name, g, nat = case
+    nat.refresh_history(g["primary"], g["phase_state"])
+    cur = torch.as_tensor(g["current"], device="cuda")
+    ps = torch.as_tensor(g["phase_state"], device="cuda")
+    F = nat.form_function(cur, ps).cpu().numpy()
+    assert_entries(F, g["residual"], 1, f"{name} residual")
+    Fj = torch.empty_like(cur)
+    J = nat.assemble_jacobian(cur, ps, residual=Fj).cpu().numpy()
+    assert_entries(J, g["jacobian"], 1, f"{name} jacobian")
+    assert_entries(Fj.cpu().numpy(), g["residual"], 1, f"{name} residual from the Jacobian call")
+
+
+def test_update_state(case, torch_cuda):
+    torch = torch_cuda
+    name, g, nat = case
+    cur = torch.as_tensor(g["current"], device="cuda").clone()
+    ps = torch.as_tensor(g["phase_state"], device="cuda").clone()
+    rc, rep = nat.update_state_with_report(cur, ps)
+    assert rc == 0
+    got = np.array([getattr(rep, f) for f in REPORT_FIELDS])
+    assert np.array_equal(got, g["report"]), dict(zip(REPORT_FIELDS, zip(got, g["report"])))
+    assert_state(cur.cpu().numpy(), ps.cpu().numpy(), g["updated_primary"], g["updated_phase_state"], name)
+
+
+def test_update_state_failure_commits_nothing(case, torch_cuda):
+    torch = torch_cuda
+    name, g, nat = case
+    cur = torch.as_tensor(g["failing"], device="cuda").clone()
+    ps = torch.as_tensor(g["phase_state"], device="cuda").clone()
+    before = cur.clone(), ps.clone()
+    rc, rep = nat.update_state_with_report(cur, ps)
+    assert rc == 1
+    got = np.array([getattr(rep, f) for f in REPORT_FIELDS])
+    assert np.array_equal(got, g["failing_report"]), dict(zip(REPORT_FIELDS, zip(got, g["failing_report"])))
+    assert torch.equal(cur, before[0]) and torch.equal(ps, before[1])
+
+
+def test_domain_error_is_recoverable(case, torch_cuda):
+    torch = torch_cuda
+    _, g, nat = case
+    nat.refresh_history(g["primary"], g["phase_state"])
+    ps = torch.as_tensor(g["phase_state"], device="cuda").clone()
+    ps[3, 0] = 0.0   # an invalid phase-presence flag: the reference throws
+    cur = torch.as_tensor(g["current"], device="cuda")
+    with pytest.raises(FloatingPointError):
+        nat.form_function(cur, ps)
+    with pytest.raises(FloatingPointError):
+        nat.assemble_jacobian(cur, ps)
+    # the handle stays usable after the failure
+    F = nat.form_function(cur, torch.as_tensor(g["phase_state"], device="cuda")).cpu().numpy()
+    assert_entries(F, g["residual"], 1, "residual after a domain error")
+
+
+def test_bad_topology_is_rejected(torch_cuda):
+    from nonenone_b200.lib import NzError
+    grid, _, _ = synth.natural_case(0, nx=4, ny=3, nz=1)
+    one_way = types.SimpleNamespace(**{k: getattr(grid, k) for k in (
+        "ncell", "porosity", "volume", "conn_offset", "conn_neighbor", "conn_trans", "conn_gravity")})
+    one_way.conn_neighbor = grid.conn_neighbor.copy()
+    one_way.conn_neighbor[0] = 5   # cell 0 -> 5 has no reverse connection
+    with pytest.raises(NzError):
+        assembler(make_fluid(), one_way)
+
+
+def test_full_size_parity(reference, torch_cuda):
+    """The 60x20x1 case (1200 cells, 2320 faces) against the live reference."""
+    torch = torch_cuda
+    fluid = make_fluid()
+    grid, P, z = synth.natural_case(0)
+    relperm = abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10)
+    oracle = reference.Natural(fluid, grid, 864.0, 353.15, relperm)
+    primary, ps = oracle.init_ptz(P, z)
+    oracle.set_history(primary, ps)
+    cur = synth.perturb_natural_state(primary, ps, 3, 11, 1.0)
+    nat = assembler(fluid, grid)
+    gp, gs = nat.initialize_from_ptz(P, z)
+    assert_state(gp.cpu().numpy(), gs.cpu().numpy(), primary, ps, "init 60x20x1")
+    nat.refresh_history(primary, ps)
+    dcur = torch.as_tensor(cur, device="cuda")
+    dps = torch.as_tensor(ps, device="cuda")
+    assert_entries(nat.form_function(dcur, dps).cpu().numpy(), oracle.residual(cur, ps), 1, "residual 60x20x1")
+    assert_entries(nat.assemble_jacobian(dcur, dps).cpu().numpy(), oracle.jacobian(cur, ps), 1,
+                   "jacobian 60x20x1")
+    rc, up, ups, rep = oracle.update_state(cur, ps)
+    c2, s2 = dcur.clone(), dps.clone()
+    grc, grep = nat.update_state_with_report(c2, s2)
+    assert grc == rc
+    assert [getattr(grep, f) for f in REPORT_FIELDS] == [getattr(rep, f) for f in REPORT_FIELDS]
+    assert_state(c2.cpu().numpy(), s2.cpu().numpy(), up, ups, "update 60x20x1")
