@@ -15,6 +15,10 @@ seeded synthetic mixture of roughly 40/40/20 % single/two/three-phase points
   cpu_baseline  the reference's own FP64 flash (oracle/_ref, compiled from the
          reference tree) on a bounded sample, all host threads
 
+natural  one Natural Newton evaluation (phase-state update + residual + BAIJ
+         Jacobian) on the 60x20x1 case beside the reference's own loops on one
+         core, and on a 2,000,000-cell grid with the Jacobian's HBM roofline
+
 --impl reference times that reference CPU flash alone (rank 0; other ranks
 exit).  With --gpus N under torchrun every rank flashes its own batch (weak
 scaling, no collective on the data path); the time is the max over ranks.
@@ -125,6 +129,115 @@ def cpu_reference_rate(fluid, P, T, z, seconds_target: float = 15.0):
                       f"shuffled, so the sample has the workload's label mix); "
                       f"{threads} threads, one CubicThreePhaseFlash each; {dt:.1f} s",
             "single_core_us_per_flash": per_point * 1e6}
+
+
+def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: bool):
+    """One Natural Newton evaluation (transactional phase-state update of a
+    perturbed iterate + residual + BAIJ Jacobian) on two grids:
+
+    * the 60x20x1 H2O/CO2/nC10 case (1200 cells, 2320 faces), beside the
+      reference's own loops on one host core (the reference runtime is one
+      thread per MPI rank);
+    * a 200x200x50 grid (2,000,000 cells, 5.94 M faces) of the same fluid, for
+      the Jacobian's HBM roofline (its values are written once, 100 doubles per
+      block: algorithmic bytes = blocks x B^2 x 8 + residual).
+    """
+    import torch
+    from nonenone_b200 import abi, synth
+    from nonenone_b200.flash import CubicThreePhaseFlash, Context
+    from nonenone_b200.fluids import make_fluid
+    from nonenone_b200.natural import NaturalAssembler
+    relperm = abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10)
+    fluid = make_fluid()
+    results = {}
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        a, b = events()
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    for label, shape in (("60x20x1", (60, 20, 1)), ("200x200x50", (200, 200, 50))):
+        grid, P, z = synth.natural_case(0, nx=shape[0], ny=shape[1], nz=shape[2])
+        ctx = Context(fluid, device=local)
+        nat = NaturalAssembler(ctx, grid, 864.0, 353.15, relperm)
+        # cells whose P-T-z flash the reference cannot converge (a few per
+        # million) take a converged cell's inputs, so the initial state exists
+        fl = CubicThreePhaseFlash(fluid, device=local)
+        st = fl.flash(P, np.full(grid.ncell, 353.15), np.ascontiguousarray(z.T),
+                      precision=abi.PRECISION_FP64_STAGED)["status"].cpu().numpy()
+        bad, good = np.where(st != 0)[0], np.where(st == 0)[0]
+        P, z = P.copy(), z.copy()
+        P[bad], z[bad] = P[good[:bad.size]], z[good[:bad.size]]
+        primary, ps = nat.initialize_from_ptz(P, z)
+        nat.refresh_history(primary, ps)
+        cur_np = synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), NC, 11, 1.0)
+        cur = torch.as_tensor(cur_np, device=primary.device)
+        F = torch.empty_like(cur)
+        vals = torch.empty(nat.nnzb, nat.B, nat.B, dtype=torch.float64, device=primary.device)
+        work_p, work_s = cur.clone(), ps.clone()
+
+        def update():
+            work_p.copy_(cur)
+            work_s.copy_(ps)
+            return nat.update_state_with_report(work_p, work_s)
+
+        def newton():
+            update()
+            nat.form_function(cur, ps, out=F)
+            nat.assemble_jacobian(cur, ps, values=vals)
+
+        n_rep = reps if grid.ncell <= 10000 else 1
+        newton()   # warm-up
+        torch.cuda.synchronize()
+        t_update = sorted(timed(update) for _ in range(n_rep))
+        t_res = sorted(timed(lambda: nat.form_function(cur, ps, out=F)) for _ in range(max(n_rep, 3)))
+        t_jac = sorted(timed(lambda: nat.assemble_jacobian(cur, ps, values=vals)) for _ in range(max(n_rep, 3)))
+        t_newton = sorted(timed(newton) for _ in range(n_rep))
+        rc, rep = update()
+        jac_bytes = nat.nnzb * nat.B * nat.B * 8 + grid.ncell * nat.B * 8
+        jac_ms = t_jac[len(t_jac) // 2]
+        entry = {
+            "cells": grid.ncell, "faces": int(grid.nfaces), "block": nat.B, "blocks": nat.nnzb,
+            "newton_eval_ms": {"p50": t_newton[len(t_newton) // 2], "max": t_newton[-1], "reps": n_rep},
+            "cell_evals_per_s": grid.ncell / (t_newton[len(t_newton) // 2] * 1e-3),
+            "update_ms": t_update[len(t_update) // 2],
+            "residual_ms": t_res[len(t_res) // 2],
+            "jacobian_ms": jac_ms,
+            "update_committed": rc == 0,
+            "stable_reduced_cells": int(rep.stable_reduced_cells),
+            "jacobian_roofline": {"bound": "hbm", "bytes_per_launch": jac_bytes,
+                                  "achieved": jac_bytes / (jac_ms * 1e-3) / 1e9, "unit": "GB/s",
+                                  "peak": hbm_peak,
+                                  "frac": (jac_bytes / (jac_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None},
+        }
+        if with_cpu and label == "60x20x1":
+            try:
+                from oracle import ref
+                if ref.available():
+                    oracle = ref.Natural(fluid, grid, 864.0, 353.15, relperm)
+                    p0, s0 = primary.cpu().numpy(), ps.cpu().numpy()
+                    oracle.set_history(p0, s0)
+                    t0 = time.perf_counter()
+                    oracle.update_state(cur_np, s0)
+                    oracle.residual(cur_np, s0)
+                    oracle.jacobian(cur_np, s0)
+                    dt = time.perf_counter() - t0
+                    entry["cpu_reference"] = {
+                        "newton_eval_ms": dt * 1e3, "cell_evals_per_s": grid.ncell / dt, "cores": 1,
+                        "kind": "reference", "what": "the reference's updatePhaseState / residual / "
+                                                    "Jacobian loops (oracle/_ref), one thread, same state"}
+            except Exception as ex:
+                entry["cpu_reference"] = {"error": str(ex)}
+        results[label] = entry
+        del nat, ctx, fl, vals
+        torch.cuda.empty_cache()
+    return results
 
 
 def run_reference(args):
@@ -308,7 +421,19 @@ def run_gpu(args):
     peak = fp64.value if precision != abi.PRECISION_MIXED else fp32.value
     status = slots[0]["out"]["status"].cpu().numpy()
     presence = slots[0]["out"]["presence"].cpu().numpy()
-    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 2 + 8 * 4 + 1
+    # staged form: start, 8 rounds x (trial, classify, 2 resume, reset), RR3 memo,
+    # recovery start, 3 recovery rounds x (trial, resume), warp recovery, 2
+    # continuation-anchor launches, select
+    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 1 + 8 * 5 + 2 + 3 * 2 + 4
+
+    natural = None
+    if rank == 0 and not args.no_natural:
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+                hbm_peak = float(json.load(fh)["hbm_gbs"])
+        except Exception:
+            hbm_peak = 6650.0
+        natural = natural_measure(local, 5, hbm_peak, not args.no_cpu_baseline)
 
     if rank == 0:
         cpu = None
@@ -357,6 +482,7 @@ def run_gpu(args):
             "clocks": clocks.summary(),
             "fp32_fma_peak_tflops": fp32.value,
             "cpu_baseline": cpu,
+            "natural": natural,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -374,6 +500,8 @@ def main():
     ap.add_argument("--precision", default="fp64_staged", choices=["fp64", "fp64_staged", "mixed"])
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-natural", action="store_true",
+                    help="skip the Natural Newton-evaluation measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -60,6 +60,11 @@ struct Result
     }
 };
 
+// Outcome of one pressure-continuation anchor.
+constexpr int CONT_NONE = 0;
+constexpr int CONT_SUCCESS = 1;
+constexpr int CONT_ERROR = 2;
+
 template <int NC>
 struct StabilityResult
 {
@@ -199,6 +204,29 @@ NZ_HDI void swRolePermutation(int k, int (&roles)[3])
     roles[2] = table[k][2];
 }
 
+// A robust three-phase Rachford-Rice answer computed ahead of time for one
+// exact input (z, K_g, K_w and the preferred fractions).  rr3Robust returns it
+// when it is called with bit-identical inputs and solves as usual otherwise.
+template <int NC>
+struct Rr3Memo
+{
+    double z[NC], kg[NC], kw[NC];
+    double pg, pw;
+    double bg, bw;
+    int ok;
+    int valid;
+
+    NZ_HD bool matches(const double *zz, const double *g, const double *w, double ppg, double ppw) const
+    {
+        if (!valid || pg != ppg || pw != ppw)
+            return false;
+        for (int i = 0; i < NC; ++i)
+            if (z[i] != zz[i] || kg[i] != g[i] || kw[i] != w[i])
+                return false;
+        return true;
+    }
+};
+
 // ============================================================================
 template <int NC>
 struct Solver
@@ -219,6 +247,7 @@ struct Solver
     double cacheP, cacheT;
     MixParams<NC> nonAq;
     MixParams<NC> aq;
+    const Rr3Memo<NC> *memo;   // optional precomputed rr3Robust answer
 
     NZ_HD void setup(const FluidDev *fluid, double s)
     {
@@ -233,6 +262,7 @@ struct Solver
         width = 1;
         cacheValid = false;
         cacheP = cacheT = 0.0;
+        memo = nullptr;
     }
 
     NZ_HD const FlashOpts &O() const { return F->opt; }
@@ -434,6 +464,44 @@ struct Solver
             {1.0e-4, 0.80}, {0.20, 0.20}, {0.60, 0.20}, {0.20, 0.60}, {0.05, 0.05},
             {0.90, 0.01}, {0.95, 1.0e-4}, {0.98, 1.0e-4}, {1.0e-4, 0.95}, {1.0e-4, 0.98},
             {0.01, 0.90}, {0.45, 0.45}};
+        if (memo && memo->matches(z, kg, kw, pg, pw))
+        {
+            if (!memo->ok)
+                return false;
+            bg = memo->bg;
+            bw = memo->bw;
+            return true;
+        }
+#ifdef __CUDA_ARCH__
+        if (width > 1)
+        {
+            // Warp-cooperative: the preferred start on every lane (it usually
+            // converges), then the other 16 starts spread over the lanes.  Each
+            // start is an independent deterministic solve, so taking the lowest
+            // converged start reproduces the sequential first-success rule.
+            if (rr3(z, kg, kw, guesses[0][0], guesses[0][1], bg, bw))
+                return true;
+            int found = 0x7fffffff;
+            double lg = 0.0, lw = 0.0;
+#pragma unroll 1
+            for (int g = 1 + lane; g < 17; g += width)
+                if (rr3(z, kg, kw, guesses[g][0], guesses[g][1], lg, lw))
+                {
+                    found = g;
+                    break;
+                }
+            __syncwarp();
+            int first = found;
+            for (int off = 16; off > 0; off >>= 1)
+                first = imin(first, __shfl_xor_sync(0xffffffffu, first, off));
+            if (first == 0x7fffffff)
+                return false;
+            const int src = (first - 1) % width;
+            bg = __shfl_sync(0xffffffffu, lg, src);
+            bw = __shfl_sync(0xffffffffu, lw, src);
+            return true;
+        }
+#endif
 #pragma unroll 1
         for (int g = 0; g < 17; ++g)
             if (rr3(z, kg, kw, guesses[g][0], guesses[g][1], bg, bw))
@@ -3148,7 +3216,22 @@ struct Solver
         }
         if (err)
             return;
+        recover<TopLevel>(P, T, z, out);
+    }
+
+    // The fail-only recoveries of flash() (three_phase_flash.hpp:122-224), run
+    // when the active-set path did not give an accepted result.  On entry out
+    // holds that failed result (converged == false) and z is normalised; out is
+    // replaced by the first recovery that succeeds.  `from` > 1 skips the
+    // recoveries before it (they already ran and failed).
+    template <bool TopLevel>
+    NZ_HDN void recover(double P, double T, const double *z, Result<NC> &out, int from = 1)
+    {
+        double kg[NC], kw[NC];
+        wilsonK(P, T, kg);
+        initialWaterK(kw);
         // recovery 1: direct three-phase solve
+        if (from <= 1)
         {
             Result<NC> full;
             flashThree(P, T, z, kg, kw, full);
@@ -3170,6 +3253,7 @@ struct Solver
         if (err)
             return;
         // recovery 2: stable reduced phase sets
+        if (from <= 2)
         {
             Result<NC> reduced;
             stableReducedSetFallback(P, T, z, reduced);
@@ -3256,82 +3340,98 @@ struct Solver
         {
             Result<NC> continued;
             pressureContinuation(P, T, z, continued);
-            if (continued.converged)
-            {
-                canonicalizeFinal(P, T, continued, false);
-                if (continued.converged && validatePhysical(P, T, z, continued))
-                {
-                    preferStableSwReducedOverSingle(P, T, z, continued);
-                    if (continued.converged)
-                    {
-                        out = continued;
-                        return;
-                    }
-                }
-            }
+            acceptContinued(P, T, z, continued, out);
         }
     }
 
-    // pressureContinuationFallback_ (restricted.inc:554-627)
+    // One anchor of pressureContinuationFallback_ (restricted.inc:554-627): the
+    // anchor flash at P * ratio[a], then the log-pressure path to P seeded by it.
+    // Returns CONT_NONE (anchor or path did not converge), CONT_SUCCESS (out
+    // holds the continued result) or CONT_ERROR (err is set).  Anchors are
+    // independent of one another, so they may run in any order or in parallel;
+    // the fallback's answer is that of the first anchor that is not CONT_NONE.
+    NZ_HDN int continuationAnchor(double P, double T, const double *z, int a, Result<NC> &out)
+    {
+        const double ratios[8] = {0.95, 1.05, 0.90, 1.10, 0.80, 1.25, 0.65, 1.50};
+        const double anchorP = P * ratios[a];
+        if (!(anchorP > 0.0) || !isfinite(anchorP))
+            return CONT_NONE;
+        Result<NC> anchor, current;
+        {
+            Solver<NC> nested = *this;
+            nested.permutationSearch = false;
+            nested.continuation = false;
+            nested.template flash<false>(anchorP, T, z, anchor);
+            evals = nested.evals;
+            if (nested.err)
+            {
+                fail(nested.err);
+                return CONT_ERROR;
+            }
+        }
+        if (!anchor.converged)
+            return CONT_NONE;
+        numericalSwRoleResult(anchor, out);
+        if (!out.converged || out.presence == 0)
+            return CONT_NONE;
+        const double logTarget = log(P);
+        const double logAnchor = log(anchorP);
+        const double logSpan = fabs(logTarget - logAnchor);
+        int steps = int(ceil(logSpan / 0.025));
+        steps = steps < 1 ? 1 : (steps > 12 ? 12 : steps);
+        int totalIterations = anchor.iterations;
+#pragma unroll 1
+        for (int s = 1; s <= steps; ++s)
+        {
+            const double fraction = double(s) / steps;
+            const double stepP = exp(logAnchor + fraction * (logTarget - logAnchor));
+            equilibrateActiveSet(stepP, T, z, out.presence, out, false, current);
+            if (err)
+                return CONT_ERROR;
+            if (!current.converged)
+                return CONT_NONE;
+            totalIterations += current.iterations;
+            out = current;
+        }
+        if (!out.converged)
+            return CONT_NONE;
+        out.iterations = totalIterations;
+        return CONT_SUCCESS;
+    }
+
+    // pressureContinuationFallback_ (restricted.inc:554-627): anchors in order.
     NZ_HDN void pressureContinuation(double P, double T, const double *z, Result<NC> &out)
     {
         out.init();
         if (!(P > 0.0))
             return;
-        const double ratios[8] = {0.95, 1.05, 0.90, 1.10, 0.80, 1.25, 0.65, 1.50};
-        const double logTarget = log(P);
-        Result<NC> anchor, seed, current;
+        Result<NC> continued;
 #pragma unroll 1
         for (int a = 0; a < 8; ++a)
         {
-            const double anchorP = P * ratios[a];
-            if (!(anchorP > 0.0) || !isfinite(anchorP))
-                continue;
+            const int outcome = continuationAnchor(P, T, z, a, continued);
+            if (outcome == CONT_ERROR)
+                return;
+            if (outcome == CONT_SUCCESS)
             {
-                Solver<NC> nested = *this;
-                nested.permutationSearch = false;
-                nested.continuation = false;
-                nested.template flash<false>(anchorP, T, z, anchor);
-                evals = nested.evals;
-                if (nested.err)
-                {
-                    fail(nested.err);
-                    return;
-                }
-            }
-            if (!anchor.converged)
-                continue;
-            numericalSwRoleResult(anchor, seed);
-            if (!seed.converged || seed.presence == 0)
-                continue;
-            const double logAnchor = log(anchorP);
-            const double logSpan = fabs(logTarget - logAnchor);
-            int steps = int(ceil(logSpan / 0.025));
-            steps = steps < 1 ? 1 : (steps > 12 ? 12 : steps);
-            int totalIterations = anchor.iterations;
-            bool pathConverged = true;
-#pragma unroll 1
-            for (int s = 1; s <= steps; ++s)
-            {
-                const double fraction = double(s) / steps;
-                const double stepP = exp(logAnchor + fraction * (logTarget - logAnchor));
-                equilibrateActiveSet(stepP, T, z, seed.presence, seed, false, current);
-                if (err)
-                    return;
-                if (!current.converged)
-                {
-                    pathConverged = false;
-                    break;
-                }
-                totalIterations += current.iterations;
-                seed = current;
-            }
-            if (pathConverged && seed.converged)
-            {
-                seed.iterations = totalIterations;
-                out = seed;
+                out = continued;
                 return;
             }
+        }
+    }
+
+    // What flash() does with a continued result (three_phase_flash.hpp:206-224):
+    // out is replaced only when the result survives the final checks.
+    NZ_HDN void acceptContinued(double P, double T, const double *z, Result<NC> &continued, Result<NC> &out)
+    {
+        if (!continued.converged)
+            return;
+        canonicalizeFinal(P, T, continued, false);
+        if (continued.converged && validatePhysical(P, T, z, continued))
+        {
+            preferStableSwReducedOverSingle(P, T, z, continued);
+            if (continued.converged)
+                out = continued;
         }
     }
 };

@@ -13,6 +13,7 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
 {
     const int64_t n = a.g.ncell;
     const unsigned grid = unsigned((n + kNatBlock - 1) / kNatBlock);
+    const unsigned warpGrid = unsigned((n * 32 + kNatBlock - 1) / kNatBlock);   // one warp per cell
     switch (op)
     {
     case NAT_CACHE:
@@ -34,11 +35,11 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
         natHistoryKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.prevAcc, a.flag);
         break;
     case NAT_UPDATE:
-        natUpdateKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, n, a.primary, a.ps, a.newPrimary, a.newPs,
+        natUpdateKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.primary, a.ps, a.newPrimary, a.newPs,
                                                        a.status, a.firstFailure);
         break;
     case NAT_INIT:
-        natInitKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
+        natInitKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
                                                      a.firstFailure);
         break;
     default:

@@ -222,9 +222,11 @@ NZ_BOTH uint8_t packOutcome(const UpdateOutcome &o)
 }
 
 // sanitizePrimaryBeforeFlash + updatePhaseState of cell c into the scratch copy.
+// With width > 1, `width` lanes run the cell in lockstep and split the seeds of
+// its stability tests; lane 0 writes.
 template <int NC>
 NZ_HD uint8_t cellUpdate(const FluidDev &F, const NatConst &K, const double *primary, const double *ps, int64_t c,
-                         double *newPrimary, double *newPs)
+                         double *newPrimary, double *newPs, int lane = 0, int width = 1)
 {
     using L = Layout<NC>;
     double a[L::B];
@@ -235,12 +237,14 @@ NZ_HD uint8_t cellUpdate(const FluidDev &F, const NatConst &K, const double *pri
         return packOutcome(UpdateOutcome{UPD_FAILED, false, false, false, false, false});
     Equilibrium<NC> eq;
     eq.s.setup(&F, F.salinity);
+    eq.s.lane = lane;
+    eq.s.width = width;
     eq.K = &K;
     eq.sanitize(a);
     UpdateOutcome o = eq.update(a, rec);
     if (eq.s.err)
         o = UpdateOutcome{UPD_FAILED, false, false, false, false, false};
-    if (o.status != UPD_FAILED)
+    if (o.status != UPD_FAILED && lane == 0)
     {
         for (int r = 0; r < L::B; ++r)
             newPrimary[c * L::B + r] = a[r];
@@ -254,11 +258,13 @@ NZ_HD uint8_t cellUpdate(const FluidDev &F, const NatConst &K, const double *pri
 // flash does not converge (the reference throws).
 template <int NC>
 NZ_HD bool cellInitPtz(const FluidDev &F, const NatConst &K, const double *P, const double *z, int64_t c,
-                       double *primary, double *ps)
+                       double *primary, double *ps, int lane = 0, int width = 1)
 {
     using L = Layout<NC>;
     Equilibrium<NC> eq;
     eq.s.setup(&F, F.salinity);
+    eq.s.lane = lane;
+    eq.s.width = width;
     eq.K = &K;
     Result<NC> r;
     eq.s.template flash<true>(P[c], K.temperature, z + c * NC, r);
@@ -279,6 +285,8 @@ NZ_HD bool cellInitPtz(const FluidDev &F, const NatConst &K, const double *P, co
     eq.assignFlashResult(a, rec, r);
     if (eq.s.err)
         return false;
+    if (lane != 0)
+        return true;
     for (int k = 0; k < L::B; ++k)
         primary[c * L::B + k] = a[k];
     encodePhaseRec<NC>(rec, ps + c * L::NPS);
@@ -347,6 +355,7 @@ __global__ void __launch_bounds__(kNatBlock) natHistoryKernel(const __grid_const
         atomicOr(flag, 1);
 }
 
+// One warp per cell: the lanes split the seeds of the cell's stability tests.
 template <int NC>
 __global__ void __launch_bounds__(kNatBlock) natUpdateKernel(const __grid_constant__ FluidDev F,
                                                              const __grid_constant__ NatConst K, int64_t ncell,
@@ -354,24 +363,30 @@ __global__ void __launch_bounds__(kNatBlock) natUpdateKernel(const __grid_consta
                                                              double *newPrimary, double *newPs, uint8_t *status,
                                                              unsigned long long *firstFailure)
 {
-    const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (c >= ncell)
         return;
-    const uint8_t s = cellUpdate<NC>(F, K, primary, ps, c, newPrimary, newPs);
+    const uint8_t s = cellUpdate<NC>(F, K, primary, ps, c, newPrimary, newPs, lane, 32);
+    if (lane != 0)
+        return;
     status[c] = s;
     if ((s & 3) == UPD_FAILED)
         atomicMin(firstFailure, (unsigned long long)c);
 }
+
+// One warp per cell, as the update.
 template <int NC>
 __global__ void __launch_bounds__(kNatBlock) natInitKernel(const __grid_constant__ FluidDev F,
                                                            const __grid_constant__ NatConst K, int64_t ncell,
                                                            const double *P, const double *z, double *primary,
                                                            double *ps, unsigned long long *firstFailure)
 {
-    const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (c >= ncell)
         return;
-    if (!cellInitPtz<NC>(F, K, P, z, c, primary, ps))
+    if (!cellInitPtz<NC>(F, K, P, z, c, primary, ps, lane, 32) && lane == 0)
         atomicMin(firstFailure, (unsigned long long)c);
 }
 #endif

@@ -52,6 +52,10 @@ struct DriverState
     uint8_t useConvergedSeed;
     uint8_t stage;
     uint8_t tested;
+    uint8_t mainFailed;   // the active-set path ended without an accepted result and without an error
+    uint8_t recoverFrom;  // for the warp recovery kernel: 0 = flash() from scratch, else the first recovery to run
+    uint8_t r2Cand;       // recovery 2: the candidate pair under test / next to try
+    double r2BestG;       // recovery 2: Gibbs energy of the best certified candidate (in `seed`)
 };
 
 template <int NC>
@@ -221,6 +225,116 @@ struct Driver
             res.unstable[cand] = unstable;
             res.stable = res.stable && !unstable;
         }
+        // a trial that stopped on an EOS error aborts the test, as in the
+        // sequential loop (the lowest-index error wins)
+        for (int cand = 0; cand < 3; ++cand)
+        {
+            if (active & bitOf(cand))
+                continue;
+            for (int k = 0; k < nseeds; ++k)
+                if (trials[cand * nseeds + k].valid < 0)
+                {
+                    s.fail(-trials[cand * nseeds + k].valid);
+                    return;
+                }
+        }
+    }
+
+    // ----------------------------------------------- fail-only recoveries --
+    // Recovery 1 of flash() (three_phase_flash.hpp:122-141) after a failed
+    // active-set path.  True when it decides the point: st->current is then
+    // the answer, or s.err is set.
+    NZ_HD bool recoveryOne()
+    {
+        const double P = st->P, T = st->T;
+        double kg[NC], kw[NC];
+        s.wilsonK(P, T, kg);
+        s.initialWaterK(kw);
+        Result<NC> full;
+        s.flashThree(P, T, st->z, kg, kw, full);
+        if (full.converged)
+        {
+            s.canonicalize(P, T, full);
+            s.canonicalizeFinal(P, T, full, false);
+            if (full.converged && s.validatePhysical(P, T, st->z, full))
+            {
+                s.preferStableSwReducedOverSingle(P, T, st->z, full);
+                if (full.converged)
+                {
+                    st->current = full;
+                    return true;
+                }
+            }
+        }
+        return s.err != ERR_NONE;
+    }
+
+    // stableReducedSetFallback_ (restricted.inc:655-693) as a resumable loop
+    // over the candidate pairs O+G, O+W, G+W.  Advances from pair st->r2Cand;
+    // returns STAGE_NEED_STABILITY with the stability request of that pair's
+    // candidate (held in st->lastPhysical) prepared, or STAGE_DONE when the
+    // pairs are exhausted or s.err is set.  The best certified candidate is
+    // kept in st->seed with its Gibbs energy in st->r2BestG.
+    NZ_HD uint8_t reducedAdvance()
+    {
+        const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
+        const double P = st->P, T = st->T;
+        Result<NC> &cand = st->lastPhysical;
+        while (st->r2Cand < 3)
+        {
+            s.flashRestrictedRecovery(P, T, st->z, pairs[st->r2Cand], cand);
+            if (s.err)
+                return STAGE_DONE;
+            if (cand.converged)
+            {
+                cand.presence = s.presenceFromFractions(cand.beta);
+                if (cand.presence != 0)
+                {
+                    StabilityResult<NC> direct;
+                    if (prepareStability(P, T, st->z, cand.presence, cand.x, direct))
+                        return STAGE_NEED_STABILITY;
+                    if (s.err)
+                        return STAGE_DONE;
+                    // resolved without trials: not valid, the candidate is rejected
+                }
+            }
+            ++st->r2Cand;
+        }
+        return STAGE_DONE;
+    }
+
+    // The trials of the pair under test are in: certify and rank its candidate.
+    NZ_HD void reducedCombine(const TrialOut<NC> *trials, int nseeds)
+    {
+        StabilityResult<NC> sr;
+        combineStability(trials, nseeds, sr);
+        if (s.err)
+            return;
+        if (sr.valid && sr.stable)
+        {
+            const double g = s.dimensionlessGibbs(st->P, st->T, st->lastPhysical);
+            if (isfinite(g) && g < st->r2BestG)
+            {
+                st->r2BestG = g;
+                st->seed = st->lastPhysical;
+            }
+        }
+        ++st->r2Cand;
+    }
+
+    // flash()'s acceptance of the recovery-2 answer (three_phase_flash.hpp:143-157).
+    NZ_HD bool reducedFinish()
+    {
+        Result<NC> &reduced = st->seed;
+        if (!reduced.converged)
+            return false;
+        s.canonicalizeFinal(st->P, st->T, reduced, false);
+        if (reduced.converged && s.validatePhysical(st->P, st->T, st->z, reduced))
+        {
+            st->current = reduced;
+            return true;
+        }
+        return false;
     }
 
     // equilibrateActiveSet_ as a resumable loop (allocation.inc:707-858).
@@ -381,6 +495,9 @@ struct Driver
                     return STAGE_DONE;
             }
         }
+        // flash() marks the failed result and goes on to its recoveries
+        selected.converged = false;
+        st->mainFailed = s.err == ERR_NONE;
         return STAGE_NEED_FULL;
     }
 
@@ -390,6 +507,7 @@ struct Driver
         st->P = P;
         st->T = T;
         st->outer = 0;
+        st->mainFailed = 0;
         st->current.init();
         if (!s.validatePT(P, T))
             return STAGE_NEED_FULL;

@@ -66,9 +66,44 @@ struct StagedArgs
     int *full;
     int *split[2];            // resumed points: [0] finish directly, [1] continue with a new phase set
     int *counters;            // per round r: [4r]=tasks [4r+1]=pending [4r+2]=trial cursor [4r+3]=split0;
-                              // [4*kMaxRounds]=full, +1 bound flag, +2 guard flag, +3 split1 of the current round
+                              // rounds kMaxRounds.. are the recovery rounds; then full, bound flag,
+                              // guard flag, split1 of the current round, continuation queue, rest queue
+    int *cont;                // points queued for the pressure continuation
+    void *anchors;            // AnchorOut<NC>[contCap * 8]
+    int64_t contCap;
     unsigned long long *evalCounter;
 };
+
+// Per-round counters for the active-set rounds and the recovery rounds, then
+// the shared ones.
+constexpr int kRecoveryRounds = 3;   // stableReducedSetFallback_: one stability test per candidate pair
+constexpr int kRoundSlots = kMaxRounds + kRecoveryRounds;
+constexpr int kCounterFull = 4 * kRoundSlots;
+constexpr int kCounterBound = kCounterFull + 1;
+constexpr int kCounterGuard = kCounterFull + 2;
+constexpr int kCounterSplit1 = kCounterFull + 3;
+constexpr int kCounterCont = kCounterFull + 4;
+constexpr int kCounterRest = kCounterFull + 5;
+constexpr int kCounterWords = kCounterFull + 8;
+constexpr int kAnchors = 8;
+
+// Result of one pressure-continuation anchor of one point.
+template <int NC>
+struct AnchorOut
+{
+    int outcome;   // CONT_NONE / CONT_SUCCESS / CONT_ERROR
+    int err;
+    Result<NC> r;
+};
+
+// Points whose pressure continuation runs on the anchor kernels (one warp per
+// anchor); beyond this the recovery kernel runs it in place, anchor by anchor.
+inline int64_t contCapacity(int64_t n)
+{
+    if (n <= 64)
+        return n;
+    return n / 32 < 64 ? 64 : n / 32;
+}
 
 // Dispatch a point after its driver returned.
 template <int NC>
@@ -88,11 +123,11 @@ __device__ void routePoint(const StagedArgs &a, const nz_flash_out &out, int rou
     }
     else if (stage == STAGE_NEED_FULL)
     {
-        const int k = atomicAdd(&a.counters[4 * kMaxRounds], 1);
+        const int k = atomicAdd(&a.counters[kCounterFull], 1);
         if (k < a.n)
             a.full[k] = int(i);
         else
-            atomicExch(&a.counters[4 * kMaxRounds + 1], 1);
+            atomicExch(&a.counters[kCounterBound], 1);
     }
     else
     {
@@ -101,7 +136,7 @@ __device__ void routePoint(const StagedArgs &a, const nz_flash_out &out, int rou
         if (k < a.n && round < kMaxRounds)
             a.pending[q][k] = int(i);
         else
-            atomicExch(&a.counters[4 * kMaxRounds + 1], 2);
+            atomicExch(&a.counters[kCounterBound], 2);
         for (int cand = 0; cand < 3; ++cand)
             if (!(st.tested & bitOf(cand)))
             {
@@ -109,7 +144,7 @@ __device__ void routePoint(const StagedArgs &a, const nz_flash_out &out, int rou
                 if (t < 3 * a.n)
                     a.tasks[q][t] = (static_cast<unsigned long long>(i) << 2) | unsigned(cand);
                 else
-                    atomicExch(&a.counters[4 * kMaxRounds + 1], 3);
+                    atomicExch(&a.counters[kCounterBound], 3);
             }
     }
 }
@@ -157,7 +192,7 @@ stagedClassifyKernel(const __grid_constant__ FluidDev F, const __grid_constant__
         const int64_t i = a.pending[q][k];
         if (i < 0 || i >= a.n)
         {
-            atomicExch(&a.counters[4 * kMaxRounds + 1], 4);
+            atomicExch(&a.counters[kCounterBound], 4);
             continue;
         }
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
@@ -166,16 +201,17 @@ stagedClassifyKernel(const __grid_constant__ FluidDev F, const __grid_constant__
         d.st = &states[i];
         d.s.setup(&F, d.st->sal);
         d.combineStability(trials, nseeds, d.st->sr);
+        d.st->err = d.s.err;   // a trial error ends the active-set path on resume
         bool adds = false;
         if (d.st->sr.valid && !d.st->sr.stable)
             for (int p = 0; p < 3; ++p)
                 adds = adds || (!(d.st->tested & bitOf(p)) && d.st->sr.unstable[p]);
         const int which = adds ? 1 : 0;
-        const int slot = atomicAdd(which ? &a.counters[4 * kMaxRounds + 3] : &a.counters[4 * round + 3], 1);
+        const int slot = atomicAdd(which ? &a.counters[kCounterSplit1] : &a.counters[4 * round + 3], 1);
         if (slot < a.n)
             a.split[which][slot] = int(i);
         else
-            atomicExch(&a.counters[4 * kMaxRounds + 1], 7);
+            atomicExch(&a.counters[kCounterBound], 7);
     }
 }
 
@@ -184,20 +220,21 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                    const __grid_constant__ nz_flash_out out, int round, int which)
 {
-    const int count = which ? a.counters[4 * kMaxRounds + 3] : a.counters[4 * round + 3];
+    const int count = which ? a.counters[kCounterSplit1] : a.counters[4 * round + 3];
     unsigned long long evals = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count && k < a.n; k += gridDim.x * blockDim.x)
     {
         const int64_t i = a.split[which][k];
         if (i < 0 || i >= a.n)
         {
-            atomicExch(&a.counters[4 * kMaxRounds + 1], 4);
+            atomicExch(&a.counters[kCounterBound], 4);
             continue;
         }
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
         Driver<NC> d;
         d.st = &states[i];
         d.s.setup(&F, d.st->sal);
+        d.s.err = d.st->err;
         const StabilityResult<NC> sr = d.st->sr;
         const uint8_t stage = d.activeSetLoop(true, &sr);
         routePoint<NC>(a, out, round + 1, i, stage, d);
@@ -207,7 +244,7 @@ stagedResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
 }
 
 // The split-1 counter is shared by the rounds; reset it between them.
-static __global__ void stagedResetSplitKernel(int *counters) { counters[4 * kMaxRounds + 3] = 0; }
+static __global__ void stagedResetSplitKernel(int *counters) { counters[kCounterSplit1] = 0; }
 
 // Every (task, seed) TPD trial is a lane; idle lanes are refilled from the
 // round's task list with one atomic per warp.
@@ -238,7 +275,7 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
     {
         if (++guard > guardMax)
         {
-            atomicExch(&a.counters[4 * kMaxRounds + 2], 1);
+            atomicExch(&a.counters[kCounterGuard], 1);
             break;
         }
         const bool need = slot == -1;
@@ -260,7 +297,7 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                     const int cand = int(task & 3u);
                     const bool bad = point < 0 || point >= a.n || cand > 2;
                     if (bad)
-                        atomicExch(&a.counters[4 * kMaxRounds + 1], 5);
+                        atomicExch(&a.counters[kCounterBound], 5);
                     const DriverState<NC> &st = states[bad ? 0 : point];
                     evals += s.evals;
                     s.setup(&F, st.sal);
@@ -294,7 +331,8 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
             {
                 if (rc != 1 || s.err)
                 {
-                    res.valid = 0;
+                    // an EOS error is kept (as -code): it aborts the test
+                    res.valid = s.err ? -s.err : 0;
                     res.trivial = 0;
                     res.sum = 0.0;
                     for (int c = 0; c < NC; ++c)
@@ -310,6 +348,268 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
     warpAddEvals(a.evalCounter, evals);
 }
 
+// solveRr3_ (nonlinear.inc:8-96) with the line search spread over a warp: the
+// sequential loop tries lambda = 2^-l for l = 0, 1, ... 39 and takes the first
+// that lowers the norm; here lane l (and l + 32) evaluates 2^-l at once and the
+// lowest accepted l wins, which is the same step.
+template <int NC>
+__device__ bool rr3Warp(const Solver<NC> &s, const double *z, const double *kg, const double *kw, double initBg,
+                        double initBw, double &outBg, double &outBw)
+{
+    const int lane = threadIdx.x & 31;
+    double bg = sclamp(initBg, 1.0e-4, 0.8);
+    double bw = sclamp(initBw, 1.0e-4, 0.8);
+    if (bg + bw >= 0.95)
+    {
+        const double scale = 0.8 / (bg + bw);
+        bg *= scale;
+        bw *= scale;
+    }
+    for (int it = 0; it < s.O().maxRr; ++it)
+    {
+        double fg, fw, jgg, jww, jgw;
+        const double norm = s.rr3Norm(z, kg, kw, bg, bw, fg, fw, jgg, jww, jgw);
+        if (!isfinite(norm))
+            return false;
+        if (norm < s.O().rrTol)
+        {
+            outBg = bg;
+            outBw = bw;
+            return true;
+        }
+        const double det = jgg * jww - jgw * jgw;
+        if (fabs(det) < 1.0e-24 || !isfinite(det))
+            return false;
+        const double dbg = (-fg * jww + fw * jgw) / det;
+        const double dbw = (-fw * jgg + fg * jgw) / det;
+        bool accepted = false;
+        for (int base = 0; base < 40 && !accepted; base += 32)
+        {
+            const int l = base + lane;
+            bool ok = false;
+            double cg = 0.0, cw = 0.0;
+            if (l < 40)
+            {
+                const double lambda = ldexp(1.0, -l);
+                cg = bg + lambda * dbg;
+                cw = bw + lambda * dbw;
+                double a, b, c, d, e;
+                const double cn = s.rr3Norm(z, kg, kw, cg, cw, a, b, c, d, e);
+                ok = isfinite(cn) && cn < norm;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (m)
+            {
+                const int src = __ffs(m) - 1;
+                bg = __shfl_sync(0xffffffffu, cg, src);
+                bw = __shfl_sync(0xffffffffu, cw, src);
+                accepted = true;
+            }
+        }
+        if (!accepted)
+            return false;
+    }
+    return false;
+}
+
+// The first robust RR3 of recovery 1 (flashThree from Wilson K_g and the
+// initial K_w, fractions 0.15 / 0.15), one warp per point, starts in
+// solveRr3Robust_'s order.  The answer is kept as the point's Rr3Memo, in its
+// trial slots (unused until recovery 2 queues trials).
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedRr3MemoKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
+{
+    const int count = a.counters[kCounterFull];
+    const int nseeds = seedCount<NC>(F);
+    const int lane = threadIdx.x & 31;
+    const int64_t warpId = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const double guesses[17][2] = {
+        {0.15, 0.15}, {0.333, 0.333}, {0.50, 1.0e-4}, {1.0e-4, 0.50}, {0.80, 1.0e-4},
+        {1.0e-4, 0.80}, {0.20, 0.20}, {0.60, 0.20}, {0.20, 0.60}, {0.05, 0.05},
+        {0.90, 0.01}, {0.95, 1.0e-4}, {0.98, 1.0e-4}, {1.0e-4, 0.95}, {1.0e-4, 0.98},
+        {0.01, 0.90}, {0.45, 0.45}};
+    for (int64_t k = warpId; k < count && k < a.n; k += nwarps)
+    {
+        const int64_t i = a.full[k];
+        if (i < 0 || i >= a.n)
+            continue;
+        const DriverState<NC> &st = static_cast<const DriverState<NC> *>(a.states)[i];
+        if (!st.mainFailed)
+            continue;
+        Solver<NC> s;
+        s.setup(&F, st.sal);
+        Rr3Memo<NC> m;
+        double kg[NC], kw[NC];
+        s.wilsonK(st.P, st.T, kg);
+        s.initialWaterK(kw);
+        for (int c = 0; c < NC; ++c)
+        {
+            m.z[c] = st.z[c];
+            m.kg[c] = sclamp(kg[c], 1.0e-100, 1.0e100);
+            m.kw[c] = sclamp(kw[c], 1.0e-100, 1.0e100);
+        }
+        m.pg = m.pw = 0.15;
+        m.ok = 0;
+        m.bg = m.bw = 0.0;
+        for (int g = 0; g < 17 && !m.ok; ++g)
+            m.ok = rr3Warp<NC>(s, m.z, m.kg, m.kw, g == 0 ? m.pg : guesses[g][0], g == 0 ? m.pw : guesses[g][1],
+                               m.bg, m.bw) ? 1 : 0;
+        m.valid = 1;
+        if (lane == 0)
+            *reinterpret_cast<Rr3Memo<NC> *>(static_cast<TrialOut<NC> *>(a.trials) + i * 3 * nseeds) = m;
+    }
+}
+
+// Where a point goes after a recovery step (recovery rounds are numbered from
+// kMaxRounds): more trials, an answer, an error, or the warp recovery kernel.
+template <int NC>
+__device__ void routeRecovery(const StagedArgs &a, const nz_flash_out &out, int rr, int64_t i, uint8_t stage,
+                              Driver<NC> &d)
+{
+    DriverState<NC> &st = *d.st;
+    if (stage == STAGE_NEED_STABILITY && rr < kRecoveryRounds)
+    {
+        const int round = kMaxRounds + rr;
+        const int q = round & 1;
+        const int k = atomicAdd(&a.counters[4 * round + 1], 1);
+        if (k < a.n)
+            a.pending[q][k] = int(i);
+        else
+            atomicExch(&a.counters[kCounterBound], 9);
+        for (int cand = 0; cand < 3; ++cand)
+            if (!(st.tested & bitOf(cand)))
+            {
+                const int t = atomicAdd(&a.counters[4 * round], 1);
+                if (t < 3 * a.n)
+                    a.tasks[q][t] = (static_cast<unsigned long long>(i) << 2) | unsigned(cand);
+                else
+                    atomicExch(&a.counters[kCounterBound], 10);
+            }
+        return;
+    }
+    if (stage == STAGE_NEED_STABILITY)   // more pairs than rounds: cannot happen (3 pairs, 3 rounds)
+        atomicExch(&a.counters[kCounterBound], 11);
+    if (d.s.err)
+    {
+        Result<NC> failed;
+        failed.init();
+        writeFlashOut<NC>(out, a.n, i, failed, uint8_t(d.s.err));
+        return;
+    }
+    if (d.reducedFinish())
+    {
+        if (d.s.err)
+        {
+            Result<NC> failed;
+            failed.init();
+            writeFlashOut<NC>(out, a.n, i, failed, uint8_t(d.s.err));
+        }
+        else
+            writeFlashOut<NC>(out, a.n, i, st.current, NZ_FLASH_CONVERGED);
+        return;
+    }
+    st.recoverFrom = 3;
+    const int k = atomicAdd(&a.counters[kCounterRest], 1);
+    if (k < a.n)
+        a.split[0][k] = int(i);
+    else
+        atomicExch(&a.counters[kCounterBound], 12);
+}
+
+// Points whose active-set path failed: flash()'s recovery 1, then recovery 2
+// up to its first stability test.  Points that failed for another reason
+// (an error, too many rounds) go to the warp recovery kernel whole.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedRecoverStartKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
+                         const __grid_constant__ nz_flash_out out)
+{
+    const int count = a.counters[kCounterFull];
+    unsigned long long evals = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count && k < a.n; k += gridDim.x * blockDim.x)
+    {
+        const int64_t i = a.full[k];
+        if (i < 0 || i >= a.n)
+        {
+            atomicExch(&a.counters[kCounterBound], 6);
+            continue;
+        }
+        DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+        Driver<NC> d;
+        d.st = &states[i];
+        if (!d.st->mainFailed)
+        {
+            d.st->recoverFrom = 0;
+            const int r = atomicAdd(&a.counters[kCounterRest], 1);
+            if (r < a.n)
+                a.split[0][r] = int(i);
+            else
+                atomicExch(&a.counters[kCounterBound], 12);
+            continue;
+        }
+        d.s.setup(&F, d.st->sal);
+        d.s.memo = reinterpret_cast<const Rr3Memo<NC> *>(static_cast<const TrialOut<NC> *>(a.trials) +
+                                                          i * 3 * seedCount<NC>(F));
+        const bool decided = d.recoveryOne();
+        d.s.memo = nullptr;
+        if (decided)
+        {
+            if (d.s.err)
+            {
+                Result<NC> failed;
+                failed.init();
+                writeFlashOut<NC>(out, a.n, i, failed, uint8_t(d.s.err));
+            }
+            else
+                writeFlashOut<NC>(out, a.n, i, d.st->current, NZ_FLASH_CONVERGED);
+            evals += d.s.evals;
+            continue;
+        }
+        d.st->seed.init();
+        d.st->r2BestG = nzInf();
+        d.st->r2Cand = 0;
+        const uint8_t stage = d.reducedAdvance();
+        routeRecovery<NC>(a, out, 0, i, stage, d);
+        evals += d.s.evals;
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
+// Recovery round rr: certify the tested pair from its trials, then go on to
+// the next pair.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedRecoverResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
+                          const __grid_constant__ nz_flash_out out, int rr)
+{
+    const int round = kMaxRounds + rr;
+    const int q = round & 1;
+    const int count = a.counters[4 * round + 1];
+    const int nseeds = seedCount<NC>(F);
+    unsigned long long evals = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count && k < a.n; k += gridDim.x * blockDim.x)
+    {
+        const int64_t i = a.pending[q][k];
+        if (i < 0 || i >= a.n)
+        {
+            atomicExch(&a.counters[kCounterBound], 4);
+            continue;
+        }
+        DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+        const TrialOut<NC> *trials = static_cast<const TrialOut<NC> *>(a.trials) + i * 3 * nseeds;
+        Driver<NC> d;
+        d.st = &states[i];
+        d.s.setup(&F, d.st->sal);
+        d.reducedCombine(trials, nseeds);
+        const uint8_t stage = d.s.err ? STAGE_DONE : d.reducedAdvance();
+        routeRecovery<NC>(a, out, rr + 1, i, stage, d);
+        evals += d.s.evals;
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
 // Points whose main path did not end validated: the full solver with its
 // fail-only recoveries, one warp per point.  The lanes run the point in
 // lockstep and split the seeds of every stability test, which cuts the
@@ -319,18 +619,18 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                  const __grid_constant__ nz_flash_out out)
 {
-    const int count = a.counters[4 * kMaxRounds];
+    const int count = a.counters[kCounterRest];
     const int lane = threadIdx.x & 31;
     const int warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     unsigned long long evals = 0;
     for (int k = warpId; k < count && k < a.n; k += nwarps)
     {
-        const int64_t i = a.full[k];
+        const int64_t i = a.split[0][k];
         if (i < 0 || i >= a.n)
         {
             if (lane == 0)
-                atomicExch(&a.counters[4 * kMaxRounds + 1], 6);
+                atomicExch(&a.counters[kCounterBound], 6);
             continue;
         }
         Solver<NC> s;
@@ -341,7 +641,45 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
         for (int c = 0; c < NC; ++c)
             zi[c] = a.z[c * a.n + i];
         Result<NC> r;
-        s.template flash<true>(a.P[i], a.T[i], zi, r);
+        s.continuation = false;
+        const DriverState<NC> &ds = static_cast<const DriverState<NC> *>(a.states)[i];
+        if (ds.recoverFrom > 0)
+        {
+            // the active-set path and the first recoveries already ran (and
+            // failed) in the staged kernels: continue from that result
+            r = ds.current;
+            s.template recover<true>(a.P[i], a.T[i], ds.z, r, ds.recoverFrom);
+        }
+        else
+            s.template flash<true>(a.P[i], a.T[i], zi, r);
+        if (s.err == ERR_NONE && !r.converged)
+        {
+            // Every recovery but the pressure continuation has failed.  Queue the
+            // point for the anchor kernels (its failed result is written now and
+            // replaced there if the continuation succeeds), or, with the queue
+            // full, run the continuation here exactly as flash() would.
+            int slot = 0;
+            if (lane == 0)
+                slot = atomicAdd(&a.counters[kCounterCont], 1);
+            slot = __shfl_sync(0xffffffffu, slot, 0);
+            if (slot < a.contCap)
+            {
+                if (lane == 0)
+                {
+                    a.cont[slot] = int(i);
+                    evals += s.evals;
+                    writeFlashOut<NC>(out, a.n, i, r, NZ_FLASH_FAILED);
+                }
+                continue;
+            }
+            double zn[NC];
+            for (int c = 0; c < NC; ++c)
+                zn[c] = zi[c];
+            s.normalize(zn);
+            Result<NC> continued;
+            s.pressureContinuation(a.P[i], a.T[i], zn, continued);
+            s.acceptContinued(a.P[i], a.T[i], zn, continued, r);
+        }
         if (lane == 0)
         {
             evals += s.evals;
@@ -356,9 +694,127 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
     warpAddEvals(a.evalCounter, evals);
 }
 
+// Pressure-continuation anchors of the queued points: one warp per (point,
+// anchor), the lanes splitting the stability seeds as in the recovery kernel.
+// Launched twice: anchor 0 for every queued point (most are decided there),
+// then anchors 1..7 side by side for the points anchor 0 left undecided.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int first,
+                   int span)
+{
+    const int queued = a.counters[kCounterCont];
+    const int64_t count = queued < a.contCap ? queued : a.contCap;
+    const int lane = threadIdx.x & 31;
+    const int64_t warpId = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    AnchorOut<NC> *anchors = static_cast<AnchorOut<NC> *>(a.anchors);
+    unsigned long long evals = 0;
+    for (int64_t t = warpId; t < count * span; t += nwarps)
+    {
+        const int64_t k = t / span;
+        const int an = first + int(t % span);
+        if (first > 0 && anchors[k * kAnchors].outcome != CONT_NONE)
+            continue;   // decided by anchor 0
+        const int64_t i = a.cont[k];
+        if (i < 0 || i >= a.n)
+        {
+            if (lane == 0)
+                atomicExch(&a.counters[kCounterBound], 8);
+            continue;
+        }
+        Solver<NC> s;
+        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        s.lane = lane;
+        s.width = 32;
+        double zn[NC];
+        for (int c = 0; c < NC; ++c)
+            zn[c] = a.z[c * a.n + i];
+        s.normalize(zn);
+        Result<NC> r;
+        const int outcome = s.continuationAnchor(a.P[i], a.T[i], zn, an, r);
+        if (lane == 0)
+        {
+            AnchorOut<NC> &o = anchors[k * kAnchors + an];
+            o.outcome = outcome;
+            o.err = s.err;
+            if (outcome == CONT_SUCCESS)
+                o.r = r;
+            evals += s.evals;
+        }
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
+// The first anchor (in the fallback's order) with an outcome decides the point.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedSelectKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
+                   const __grid_constant__ nz_flash_out out)
+{
+    const int queued = a.counters[kCounterCont];
+    const int64_t count = queued < a.contCap ? queued : a.contCap;
+    const int lane = threadIdx.x & 31;
+    const int64_t warpId = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const AnchorOut<NC> *anchors = static_cast<const AnchorOut<NC> *>(a.anchors);
+    unsigned long long evals = 0;
+    for (int64_t k = warpId; k < count; k += nwarps)
+    {
+        const int64_t i = a.cont[k];
+        if (i < 0 || i >= a.n)
+            continue;
+        int chosen = -1;
+        for (int an = 0; an < kAnchors; ++an)
+            if (anchors[k * kAnchors + an].outcome != CONT_NONE)
+            {
+                chosen = an;
+                break;
+            }
+        if (chosen < 0)
+            continue;   // the failed result written by the recovery kernel stands
+        const AnchorOut<NC> &o = anchors[k * kAnchors + chosen];
+        if (o.outcome == CONT_ERROR)
+        {
+            if (lane == 0)
+            {
+                Result<NC> failed;
+                failed.init();
+                writeFlashOut<NC>(out, a.n, i, failed, uint8_t(o.err));
+            }
+            continue;
+        }
+        Solver<NC> s;
+        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        s.lane = lane;
+        s.width = 32;
+        double zn[NC];
+        for (int c = 0; c < NC; ++c)
+            zn[c] = a.z[c * a.n + i];
+        s.normalize(zn);
+        Result<NC> continued = o.r;
+        Result<NC> accepted;
+        accepted.init();
+        s.acceptContinued(a.P[i], a.T[i], zn, continued, accepted);
+        if (lane == 0)
+        {
+            evals += s.evals;
+            if (s.err != ERR_NONE)
+            {
+                accepted.init();
+                writeFlashOut<NC>(out, a.n, i, accepted, uint8_t(s.err));
+            }
+            else if (accepted.converged)
+                writeFlashOut<NC>(out, a.n, i, accepted, NZ_FLASH_CONVERGED);
+        }
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
 template <int NC>
 size_t stagedScratchBytes(int64_t n, const FluidDev &F)
 {
+    static_assert(sizeof(Rr3Memo<NC>) <= sizeof(TrialOut<NC>) * 3 * (NC + 6), "memo must fit a point's trial slots");
     const int nseeds = seedCount<NC>(F);
     size_t b = 0;
     auto add = [&](size_t bytes) { b += (bytes + 255) & ~size_t(255); };
@@ -371,7 +827,10 @@ size_t stagedScratchBytes(int64_t n, const FluidDev &F)
     add(sizeof(int) * size_t(n));
     add(sizeof(int) * size_t(n));
     add(sizeof(int) * size_t(n));
-    add(sizeof(int) * (4 * kMaxRounds + 4));
+    add(sizeof(int) * kCounterWords);
+    const int64_t cap = contCapacity(n);
+    add(sizeof(int) * size_t(cap));
+    add(sizeof(AnchorOut<NC>) * size_t(cap) * kAnchors);
     return b;
 }
 
@@ -397,7 +856,10 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
     a.full = reinterpret_cast<int *>(take(sizeof(int) * size_t(n)));
     a.split[0] = reinterpret_cast<int *>(take(sizeof(int) * size_t(n)));
     a.split[1] = reinterpret_cast<int *>(take(sizeof(int) * size_t(n)));
-    a.counters = reinterpret_cast<int *>(take(sizeof(int) * (4 * kMaxRounds + 4)));
+    a.counters = reinterpret_cast<int *>(take(sizeof(int) * kCounterWords));
+    a.contCap = contCapacity(n);
+    a.cont = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.contCap)));
+    a.anchors = take(sizeof(AnchorOut<NC>) * size_t(a.contCap) * kAnchors);
     return a;
 }
 
@@ -414,19 +876,19 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     a.z = z;
     a.sal = sal;
     a.evalCounter = evalCounter;
-    cudaMemsetAsync(a.counters, 0, sizeof(int) * (4 * kMaxRounds + 4), st);
+    cudaMemsetAsync(a.counters, 0, sizeof(int) * kCounterWords, st);
     const bool check = stagedDebugSync();
     auto after = [&](const char *what, int round) {
         if (!check)
             return 0;
         cudaError_t e = cudaStreamSynchronize(st);
-        int c[4 * kMaxRounds + 4];
+        int c[kCounterWords];
         cudaMemcpy(c, a.counters, sizeof(c), cudaMemcpyDeviceToHost);
-        fprintf(stderr, "[staged] %s round %d: %s tasks=%d pending=%d full=%d bound=%d guard=%d\n", what, round,
-                cudaGetErrorString(e), c[4 * (round < kMaxRounds ? round : 0)],
-                c[4 * (round < kMaxRounds ? round : 0) + 1], c[4 * kMaxRounds], c[4 * kMaxRounds + 1],
-                c[4 * kMaxRounds + 2]);
-        return e == cudaSuccess && c[4 * kMaxRounds + 1] == 0 && c[4 * kMaxRounds + 2] == 0 ? 0 : -1;
+        const int r = round < kRoundSlots ? round : 0;
+        fprintf(stderr, "[staged] %s round %d: %s tasks=%d pending=%d full=%d rest=%d cont=%d bound=%d guard=%d\n",
+                what, round, cudaGetErrorString(e), c[4 * r], c[4 * r + 1], c[kCounterFull], c[kCounterRest],
+                c[kCounterCont], c[kCounterBound], c[kCounterGuard]);
+        return e == cudaSuccess && c[kCounterBound] == 0 && c[kCounterGuard] == 0 ? 0 : -1;
     };
     const unsigned gridN = unsigned((n + kFlashBlock - 1) / kFlashBlock);
     stagedStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
@@ -445,9 +907,25 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         if (after("resume", round + 1))
             return setError(NZ_ERR_CUDA, "staged flash self-check failed in resume");
     }
+    stagedRr3MemoKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
+    stagedRecoverStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
+    if (after("recover", kMaxRounds))
+        return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
+    for (int rr = 0; rr < kRecoveryRounds; ++rr)
+    {
+        stagedTrialKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a, kMaxRounds + rr);
+        stagedRecoverResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, rr);
+        if (after("recover round", kMaxRounds + rr + 1))
+            return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
+    }
     stagedFullKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, out);
     if (after("full", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the full solver");
+    stagedAnchorKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, 0, 1);
+    stagedAnchorKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, 1, kAnchors - 1);
+    stagedSelectKernel<NC><<<unsigned(smCount * 2), kFlashBlock, 0, st>>>(F, a, out);
+    if (after("continuation", 0))
+        return setError(NZ_ERR_CUDA, "staged flash self-check failed in the pressure continuation");
     return 0;
 }
 

@@ -8,6 +8,12 @@ reference's own FP64 C++ (oracle/_ref/libnzref.so); the inputs are seeded
   flash_pr_nc3.npz  2048 points of the batched-flash mixture, PR
   flash_sw_nc3.npz  1024 points, Soreide-Whitson, salinity ~ U[0,2]
   flash_pr_nc6.npz  512 points, six components, PR
+  flash_continuation_pr_nc3.npz  192 points of the 1,048,576-point bench batch
+                    (synth.flash_points(2**20, seed=1)) that reach the flash's last
+                    fallback, the pressure continuation: 160 it rescues and 32 it
+                    does not (RESCUED / FAILING below, found by scanning the batch
+                    with this library's host-compiled solver with the continuation
+                    switched off; only the choice of inputs comes from that scan)
 Each holds the inputs, the full nz_flash_out record, and for converged
 points the stability trial sums of the missing phases of the final state
 (|trialSum - 1| is the distance to the phase boundary used to exclude
@@ -26,6 +32,29 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from nonenone_b200 import abi, synth  # noqa: E402
 from nonenone_b200.fluids import SIX_COMPONENT, make_fluid  # noqa: E402
 from oracle import ref  # noqa: E402
+
+
+RESCUED = (
+    187, 6787, 13970, 18453, 24723, 31078, 35682, 40026, 46128, 53689, 59326, 66687, 72474, 79984,
+    88943, 94688, 99981, 103735, 113399, 119582, 124404, 128662, 135683, 142766, 146346, 154498,
+    159325, 165215, 172093, 180023, 186797, 192793, 196887, 203081, 208501, 215626, 221446, 226343,
+    232908, 238275, 243773, 251394, 256459, 263324, 269242, 273658, 280850, 288980, 293574, 301139,
+    311750, 324317, 329344, 336068, 342327, 349748, 360265, 367787, 373327, 378244, 384988, 391227,
+    396225, 403222, 408309, 413672, 419891, 425574, 433494, 438760, 447229, 454556, 462460, 468926,
+    475364, 481293, 488043, 496799, 502081, 510908, 517967, 526451, 532261, 539193, 545951, 554840,
+    561838, 568251, 573519, 578226, 584725, 593773, 599965, 605654, 613464, 624628, 630386, 636952,
+    642374, 648314, 655679, 666178, 675259, 679812, 685584, 691809, 697421, 702248, 708573, 716886,
+    724605, 732693, 738776, 744979, 752782, 755327, 759496, 766214, 776232, 783204, 791167, 798270,
+    805079, 811706, 817122, 825149, 832689, 838979, 846530, 852708, 858652, 864868, 869100, 876423,
+    882379, 888593, 893638, 899994, 905296, 910792, 916582, 922598, 930992, 933506, 938166, 944907,
+    951407, 958644, 964378, 970957, 976391, 979846, 985294, 993079, 1000672, 1006878, 1012767,
+    1018999, 1026386, 1033423,
+)
+FAILING = (
+    2621, 10386, 18204, 28983, 41843, 100357, 123757, 141214, 156566, 192445, 215522, 222986,
+    273675, 280051, 305883, 353177, 415231, 432191, 488471, 506665, 537639, 548464, 560671, 590826,
+    609054, 629734, 644629, 672143, 680970, 735201, 759657, 773123,
+)
 
 
 def boundary_distance(fluid, P, T, z, out, salinity=None):
@@ -74,6 +103,9 @@ def main():
     T = rng.uniform(303.0, 423.0, n)
     z = np.ascontiguousarray(rng.dirichlet([4, 2, 1, 1, 1, 1], n).T)
     make("flash_pr_nc6.npz", six, P, T, z)
+    P, T, z = synth.flash_points(1 << 20, seed=1)
+    sel = np.array(RESCUED + FAILING)
+    make("flash_continuation_pr_nc3.npz", pr, P[sel], T[sel], np.ascontiguousarray(z[:, sel]))
 
 
 if __name__ == "__main__":

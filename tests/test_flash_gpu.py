@@ -118,6 +118,7 @@ def test_flash_three_phase_kat_on_gpu(torch_cuda):
     ("flash_pr_nc3.npz", dict()),
     ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
     ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
+    ("flash_continuation_pr_nc3.npz", dict()),
 ])
 def test_flash_matches_golden(torch_cuda, golden, name, fluid_args):
     from nonenone_b200.flash import CubicThreePhaseFlash
@@ -190,6 +191,7 @@ def test_stability_matches_reference(torch_cuda, reference, golden):
     ("flash_pr_nc3.npz", dict()),
     ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
     ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
+    ("flash_continuation_pr_nc3.npz", dict()),
 ])
 def test_staged_fp64_matches_golden(torch_cuda, golden, name, fluid_args):
     """The staged FP64 form (driver / trial kernels) against the reference."""

@@ -60,12 +60,17 @@ def assert_entries(gpu, ref, axis_eq, what):
     """Entry-wise check with the per-equation-row floor described above."""
     gpu = np.asarray(gpu)
     ref = np.asarray(ref)
+    # non-finite entries (where the reference's arithmetic overflows) must match exactly
+    fin = np.isfinite(ref)
+    assert np.array_equal(np.isfinite(gpu), fin), f"{what}: non-finite pattern differs"
+    inf = np.isinf(ref)
+    assert np.array_equal(gpu[inf], ref[inf]), f"{what}: infinities differ"
     assert np.array_equal(np.isnan(gpu), np.isnan(ref)), f"{what}: NaN pattern differs"
-    fin = ~np.isnan(ref)
     red = tuple(a for a in range(ref.ndim) if a != axis_eq)
-    scale = np.nanmax(np.abs(ref), axis=red, keepdims=True)
+    scale = np.max(np.where(fin, np.abs(ref), 0.0), axis=red, keepdims=True)
     denom = np.maximum(np.abs(ref), FLOOR * scale)
-    err = np.where(fin, np.abs(gpu - ref) / np.where(denom > 0, denom, 1.0), 0.0)
+    with np.errstate(invalid="ignore"):
+        err = np.where(fin, np.abs(gpu - ref) / np.where(denom > 0, denom, 1.0), 0.0)
     worst = np.unravel_index(np.argmax(err), err.shape)
     assert err.max() <= ENTRY_TOL, f"{what}: max err {err.max():.3e} at {worst}: {gpu[worst]} vs {ref[worst]}"
     return err.max()
