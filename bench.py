@@ -421,10 +421,11 @@ def run_gpu(args):
     peak = fp64.value if precision != abi.PRECISION_MIXED else fp32.value
     status = slots[0]["out"]["status"].cpu().numpy()
     presence = slots[0]["out"]["presence"].cpu().numpy()
-    # staged form: start, 8 rounds x (trial, classify, 2 resume, reset), RR3 memo,
-    # recovery start, 3 recovery rounds x (trial, resume), warp recovery, 2
-    # continuation-anchor launches, select
-    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 1 + 8 * 5 + 2 + 3 * 2 + 4
+    # staged form: start; 8 rounds x (trial, classify, 2 resume, three-phase,
+    # three-phase resume, reset); RR3 memo, recovery start, three-phase,
+    # recovery-1 accept; 3 recovery rounds x (trial, resume); warp recovery,
+    # 2 continuation-anchor launches, select
+    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 1 + 8 * 7 + 4 + 3 * 2 + 4
 
     natural = None
     if rank == 0 and not args.no_natural:

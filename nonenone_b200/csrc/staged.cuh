@@ -30,6 +30,7 @@ namespace nz
 constexpr uint8_t STAGE_DONE = 0;
 constexpr uint8_t STAGE_NEED_STABILITY = 1;
 constexpr uint8_t STAGE_NEED_FULL = 2;
+constexpr uint8_t STAGE_NEED_THREE = 3;   // suspended at a three-phase solve (flashThree_)
 
 // Per-point state kept in HBM between driver launches.
 template <int NC>
@@ -56,6 +57,8 @@ struct DriverState
     uint8_t recoverFrom;  // for the warp recovery kernel: 0 = flash() from scratch, else the first recovery to run
     uint8_t r2Cand;       // recovery 2: the candidate pair under test / next to try
     double r2BestG;       // recovery 2: Gibbs energy of the best certified candidate (in `seed`)
+    double threeKg[NC];   // starting K of the pending three-phase solve
+    double threeKw[NC];
 };
 
 template <int NC>
@@ -246,12 +249,25 @@ struct Driver
     // the answer, or s.err is set.
     NZ_HD bool recoveryOne()
     {
-        const double P = st->P, T = st->T;
         double kg[NC], kw[NC];
-        s.wilsonK(P, T, kg);
+        s.wilsonK(st->P, st->T, kg);
         s.initialWaterK(kw);
         Result<NC> full;
-        s.flashThree(P, T, st->z, kg, kw, full);
+        s.flashThree(st->P, st->T, st->z, kg, kw, full);
+        return recoveryOneAccept(full);
+    }
+
+    // The starting K of recovery 1's three-phase solve (Wilson, initial water).
+    NZ_HD void recoveryOneStart()
+    {
+        s.wilsonK(st->P, st->T, st->threeKg);
+        s.initialWaterK(st->threeKw);
+    }
+
+    // What flash() does with recovery 1's three-phase result `full`.
+    NZ_HD bool recoveryOneAccept(Result<NC> &full)
+    {
+        const double P = st->P, T = st->T;
         if (full.converged)
         {
             s.canonicalize(P, T, full);
@@ -340,7 +356,7 @@ struct Driver
     // equilibrateActiveSet_ as a resumable loop (allocation.inc:707-858).
     // Returns STAGE_NEED_STABILITY when it suspended for a stability test,
     // otherwise it has stored the loop's result in st->current.
-    NZ_HD uint8_t activeSetLoop(bool resumed, const StabilityResult<NC> *resumedSt)
+    NZ_HD uint8_t activeSetLoop(bool resumed, const StabilityResult<NC> *resumedSt, bool afterThree = false)
     {
         const double P = st->P, T = st->T;
         const double *z = st->z;
@@ -393,7 +409,19 @@ struct Driver
                 ++outer;
                 continue;
             }
-            if (useConvergedSeed)
+            if (afterThree)
+            {
+                // the three-phase solve this pass suspended at has written current
+                afterThree = false;
+                if (!current.converged)
+                {
+                    lastPhysical.converged = false;
+                    s.canonicalize(P, T, lastPhysical);
+                    current = lastPhysical;
+                    return STAGE_DONE;
+                }
+            }
+            else if (useConvergedSeed)
             {
                 current = seed;
                 useConvergedSeed = false;
@@ -428,14 +456,16 @@ struct Driver
                 }
                 if (!kgValid) s.wilsonK(P, T, kg);
                 if (!kwValid) s.initialWaterK(kw);
-                s.flashThree(P, T, z, kg, kw, current);
-                if (!current.converged)
+                // flashThree runs on the three-phase kernel; the loop resumes above
+                for (int i = 0; i < NC; ++i)
                 {
-                    lastPhysical.converged = false;
-                    s.canonicalize(P, T, lastPhysical);
-                    current = lastPhysical;
-                    return STAGE_DONE;
+                    st->threeKg[i] = kg[i];
+                    st->threeKw[i] = kw[i];
                 }
+                st->active = active;
+                st->outer = uint8_t(outer);
+                st->useConvergedSeed = useConvergedSeed;
+                return STAGE_NEED_THREE;
             }
             uint8_t fractionPresence = s.presenceFromFractions(current.beta);
             if (fractionPresence == 0)
@@ -716,6 +746,205 @@ NZ_HD int trialStep(Solver<NC> &s, TrialLane<NC> &L, TrialOut<NC> &out)
     for (int i = 0; i < NC; ++i)
         out.x[i] = t.x[i];
     return 1;
+}
+
+// ---------------------------------------------------------- three-phase --
+// flashThree_ (nonlinear.inc:279-513) as a step machine: every step is one
+// threeSsiStep or one evalThree (one robust RR3 solve and three phase
+// evaluations), so the lanes of a warp stay in step while each runs its own
+// solve.  The steps and their order are those of Solver::flashThree.
+constexpr int TH_SSI = 0;    // leading SSI steps
+constexpr int TH_BASE = 1;   // Newton base evaluation
+constexpr int TH_FD = 2;     // finite-difference column (forward, then backward if invalid)
+constexpr int TH_LINE = 3;   // line search
+constexpr int TH_TAIL = 4;   // remaining SSI budget
+
+template <int NC>
+struct ThreeLane
+{
+    static constexpr int M = 2 * NC;
+    int mode, it, ssiSteps, newtonIt, col, side, ls, total;
+    double P, T;
+    double z[NC];
+    double kg[NC], kw[NC];
+    double logK[M];
+    double bg, bw, damping;
+    double J[M][M];
+    double delta[M];
+    ThreePhaseLogKState<NC> base;
+    Result<NC> r;
+};
+
+template <int NC>
+NZ_HD void threeEnterTail(ThreeLane<NC> &L)
+{
+    L.it = L.ssiSteps;
+    L.mode = TH_TAIL;
+}
+
+template <int NC>
+NZ_HD void threeEnterNewton(ThreeLane<NC> &L)
+{
+    for (int i = 0; i < NC; ++i)
+    {
+        L.logK[i] = log(L.kg[i]);
+        L.logK[NC + i] = log(L.kw[i]);
+    }
+    L.newtonIt = 0;
+    L.mode = TH_BASE;
+}
+
+template <int NC>
+NZ_HD void threeInit(Solver<NC> &s, ThreeLane<NC> &L, const double *kgIn, const double *kwIn)
+{
+    L.r.init();
+    L.r.presence = ALL_BITS;
+    for (int i = 0; i < NC; ++i)
+    {
+        L.kg[i] = sclamp(kgIn[i], 1.0e-100, 1.0e100);
+        L.kw[i] = sclamp(kwIn[i], 1.0e-100, 1.0e100);
+    }
+    L.bg = 0.15;
+    L.bw = 0.15;
+    L.ssiSteps = imin(s.O().maxIterations, imax(s.O().threeSsi, 0));
+    L.total = 0;
+    L.it = 0;
+    L.mode = TH_SSI;
+    if (L.ssiSteps == 0)
+        threeEnterNewton(L);
+}
+
+// One step.  Returns 1 when the solve has ended: L.r is flashThree's result
+// (and s.err may be set).
+template <int NC>
+NZ_HD int threeStep(Solver<NC> &s, ThreeLane<NC> &L)
+{
+    constexpr int M = 2 * NC;
+    switch (L.mode)
+    {
+    case TH_SSI:
+        if (!s.threeSsiStep(L.P, L.T, L.z, L.kg, L.kw, L.bg, L.bw, L.total, L.r))
+            return 1;
+        if (L.r.converged || s.err)
+            return 1;
+        if (++L.it >= L.ssiSteps)
+            threeEnterNewton(L);
+        return 0;
+    case TH_BASE:
+        if (L.newtonIt >= s.O().threeNewton)
+        {
+            threeEnterTail(L);
+            return 0;
+        }
+        s.evalThree(L.P, L.T, L.z, L.logK, L.bg, L.bw, L.base);
+        if (!L.base.valid || s.err)
+        {
+            threeEnterTail(L);
+            return 0;
+        }
+        L.r = L.base.result;
+        L.r.iterations = ++L.total;
+        L.bg = L.r.beta[1];
+        L.bw = L.r.beta[2];
+        if (L.base.norm < s.O().fugacityTol)
+        {
+            L.r.converged = true;
+            L.r.presence = s.presenceFromFractions(L.r.beta);
+            s.updateSaturations(L.P, L.T, L.r);
+            return 1;
+        }
+        L.col = 0;
+        L.side = 1;
+        L.mode = TH_FD;
+        return 0;
+    case TH_FD:
+    {
+        const double step = s.O().fdStep * smax(1.0, fabs(L.logK[L.col]));
+        double pert[M];
+        for (int i = 0; i < M; ++i)
+            pert[i] = L.logK[i];
+        if (L.side > 0)
+            pert[L.col] += step;
+        else
+            pert[L.col] -= step;
+        ThreePhaseLogKState<NC> probe;
+        s.evalThree(L.P, L.T, L.z, pert, L.bg, L.bw, probe);
+        if (L.side > 0)
+        {
+            if (!probe.valid)
+            {
+                L.side = -1;
+                return 0;
+            }
+            for (int row = 0; row < M; ++row)
+                L.J[row][L.col] = (probe.residual[row] - L.base.residual[row]) / step;
+        }
+        else
+        {
+            if (!probe.valid)
+            {
+                threeEnterTail(L);
+                return 0;
+            }
+            for (int row = 0; row < M; ++row)
+                L.J[row][L.col] = (L.base.residual[row] - probe.residual[row]) / step;
+        }
+        L.side = 1;
+        if (++L.col < M)
+            return 0;
+        double rhs[M];
+        for (int i = 0; i < M; ++i)
+            rhs[i] = -L.base.residual[i];
+        if (!solveDense<M>(L.J, rhs, L.delta))
+        {
+            threeEnterTail(L);
+            return 0;
+        }
+        L.damping = 1.0;
+        L.ls = 0;
+        L.mode = TH_LINE;
+        return 0;
+    }
+    case TH_LINE:
+    {
+        double trial[M];
+        for (int i = 0; i < M; ++i)
+            trial[i] = L.logK[i] + L.damping * L.delta[i];
+        ThreePhaseLogKState<NC> probe;
+        s.evalThree(L.P, L.T, L.z, trial, L.bg, L.bw, probe);
+        if (probe.valid && probe.norm < L.base.norm)
+        {
+            for (int i = 0; i < M; ++i)
+                L.logK[i] = trial[i];
+            ++L.newtonIt;
+            L.mode = TH_BASE;
+            return 0;
+        }
+        L.damping *= 0.5;
+        if (++L.ls >= 16)
+            threeEnterTail(L);
+        return 0;
+    }
+    default:   // TH_TAIL
+        if (L.it >= s.O().maxIterations || s.err)
+            return 1;
+        for (int i = 0; i < NC; ++i)
+        {
+            L.kg[i] = exp(sclamp(L.logK[i], -230.0, 230.0));
+            L.kw[i] = exp(sclamp(L.logK[NC + i], -230.0, 230.0));
+        }
+        if (!s.threeSsiStep(L.P, L.T, L.z, L.kg, L.kw, L.bg, L.bw, L.total, L.r))
+            return 1;
+        if (L.r.converged)
+            return 1;
+        for (int i = 0; i < NC; ++i)
+        {
+            L.logK[i] = log(L.kg[i]);
+            L.logK[NC + i] = log(L.kw[i]);
+        }
+        ++L.it;
+        return 0;
+    }
 }
 
 } // namespace nz

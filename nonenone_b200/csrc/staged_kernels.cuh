@@ -68,6 +68,7 @@ struct StagedArgs
     int *counters;            // per round r: [4r]=tasks [4r+1]=pending [4r+2]=trial cursor [4r+3]=split0;
                               // rounds kMaxRounds.. are the recovery rounds; then full, bound flag,
                               // guard flag, split1 of the current round, continuation queue, rest queue
+    unsigned long long *threes;   // three-phase solves: (point << 1) | kind (0 active-set path, 1 recovery 1)
     int *cont;                // points queued for the pressure continuation
     void *anchors;            // AnchorOut<NC>[contCap * 8]
     int64_t contCap;
@@ -84,7 +85,9 @@ constexpr int kCounterGuard = kCounterFull + 2;
 constexpr int kCounterSplit1 = kCounterFull + 3;
 constexpr int kCounterCont = kCounterFull + 4;
 constexpr int kCounterRest = kCounterFull + 5;
-constexpr int kCounterWords = kCounterFull + 8;
+constexpr int kCounterThree = kCounterFull + 6;        // queued three-phase solves
+constexpr int kCounterThreeCursor = kCounterFull + 7;  // refill cursor of the three-phase kernel
+constexpr int kCounterWords = kCounterFull + 12;
 constexpr int kAnchors = 8;
 
 // Result of one pressure-continuation anchor of one point.
@@ -120,6 +123,14 @@ __device__ void routePoint(const StagedArgs &a, const nz_flash_out &out, int rou
     if (stage == STAGE_DONE)
     {
         writeFlashOut<NC>(out, a.n, i, st.current, NZ_FLASH_CONVERGED);
+    }
+    else if (stage == STAGE_NEED_THREE)
+    {
+        const int k = atomicAdd(&a.counters[kCounterThree], 1);
+        if (k < a.n)
+            a.threes[k] = static_cast<unsigned long long>(i) << 1;
+        else
+            atomicExch(&a.counters[kCounterBound], 13);
     }
     else if (stage == STAGE_NEED_FULL)
     {
@@ -243,8 +254,132 @@ stagedResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
     warpAddEvals(a.evalCounter, evals);
 }
 
-// The split-1 counter is shared by the rounds; reset it between them.
-static __global__ void stagedResetSplitKernel(int *counters) { counters[kCounterSplit1] = 0; }
+// The split-1 and three-phase counters are shared by the rounds; reset them between them.
+static __global__ void stagedResetSplitKernel(int *counters)
+{
+    counters[kCounterSplit1] = 0;
+    counters[kCounterThree] = 0;
+    counters[kCounterThreeCursor] = 0;
+}
+
+// Every queued three-phase solve is a lane running flashThree_ one step at a
+// time (ThreeLane); idle lanes are refilled with one atomic per warp.  The
+// result goes to the point's current (active-set path) or lastPhysical
+// (recovery 1) record.
+template <int NC>
+__global__ void __launch_bounds__(kTrialBlock)
+stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
+{
+    const int queued = a.counters[kCounterThree];
+    const long long total = queued < a.n ? queued : a.n;
+    int *cursor = &a.counters[kCounterThreeCursor];
+    DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+    const int nseeds = seedCount<NC>(F);
+    const unsigned lane = threadIdx.x & 31;
+    Solver<NC> s;
+    s.setup(&F, 0.0);
+    ThreeLane<NC> L;
+    long long point = -1;   // -1 idle, -2 drained
+    int kind = 0;
+    unsigned long long evals = 0;
+    // a solve takes at most ssi + newton * (1 + 4 nc + 16) + tail steps (a few
+    // hundred); the cap only guards against a wait that would never end
+    long long guard = 0;
+    const long long guardMax = 1LL << 26;
+    while (true)
+    {
+        if (++guard > guardMax)
+        {
+            atomicExch(&a.counters[kCounterGuard], 2);
+            break;
+        }
+        const bool need = point == -1;
+        const unsigned mask = __ballot_sync(0xffffffffu, need);
+        if (mask)
+        {
+            int base = 0;
+            if (lane == unsigned(__ffs(mask) - 1))
+                base = atomicAdd(cursor, __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+            if (need)
+            {
+                const long long idx = base + __popc(mask & ((1u << lane) - 1u));
+                if (idx < total)
+                {
+                    const unsigned long long task = a.threes[idx];
+                    const int64_t i = int64_t(task >> 1);
+                    if (i < 0 || i >= a.n)
+                    {
+                        atomicExch(&a.counters[kCounterBound], 14);
+                        point = -2;
+                    }
+                    else
+                    {
+                        const DriverState<NC> &st = states[i];
+                        evals += s.evals;
+                        s.setup(&F, st.sal);
+                        kind = int(task & 1u);
+                        if (kind == 1)
+                            s.memo = reinterpret_cast<const Rr3Memo<NC> *>(static_cast<const TrialOut<NC> *>(a.trials) +
+                                                                            i * 3 * nseeds);
+                        L.P = st.P;
+                        L.T = st.T;
+                        for (int c = 0; c < NC; ++c)
+                            L.z[c] = st.z[c];
+                        threeInit<NC>(s, L, st.threeKg, st.threeKw);
+                        point = i;
+                    }
+                }
+                else
+                {
+                    point = -2;
+                }
+            }
+        }
+        const bool running = point >= 0;
+        if (!__any_sync(0xffffffffu, running))
+            break;
+        if (running && threeStep<NC>(s, L))
+        {
+            DriverState<NC> &st = states[point];
+            if (kind == 1)
+                st.lastPhysical = L.r;
+            else
+                st.current = L.r;
+            st.err = s.err;
+            point = -1;
+        }
+    }
+    evals += s.evals;
+    warpAddEvals(a.evalCounter, evals);
+}
+
+// Active-set points whose three-phase solve is done: resume their loop.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedThreeResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
+                        const __grid_constant__ nz_flash_out out, int round)
+{
+    const int queued = a.counters[kCounterThree];
+    const int count = queued < a.n ? queued : int(a.n);
+    unsigned long long evals = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+    {
+        const unsigned long long task = a.threes[k];
+        const int64_t i = int64_t(task >> 1);
+        if (i < 0 || i >= a.n || (task & 1u))
+            continue;
+        DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+        Driver<NC> d;
+        d.st = &states[i];
+        d.s.setup(&F, d.st->sal);
+        d.s.err = d.st->err;
+        const uint8_t stage = d.activeSetLoop(false, nullptr, true);
+        routePoint<NC>(a, out, round + 1, i, stage, d);
+        evals += d.s.evals;
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
 
 // Every (task, seed) TPD trial is a lane; idle lanes are refilled from the
 // round's task list with one atomic per warp.
@@ -550,11 +685,40 @@ stagedRecoverStartKernel(const __grid_constant__ FluidDev F, const __grid_consta
             continue;
         }
         d.s.setup(&F, d.st->sal);
-        d.s.memo = reinterpret_cast<const Rr3Memo<NC> *>(static_cast<const TrialOut<NC> *>(a.trials) +
-                                                          i * 3 * seedCount<NC>(F));
-        const bool decided = d.recoveryOne();
-        d.s.memo = nullptr;
-        if (decided)
+        d.recoveryOneStart();
+        const int t = atomicAdd(&a.counters[kCounterThree], 1);
+        if (t < a.n)
+            a.threes[t] = (static_cast<unsigned long long>(i) << 1) | 1ull;
+        else
+            atomicExch(&a.counters[kCounterBound], 13);
+        evals += d.s.evals;
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
+// Recovery 1's three-phase solve is done: accept it, or start recovery 2 up to
+// its first stability test.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedRecoverThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
+                         const __grid_constant__ nz_flash_out out)
+{
+    const int queued = a.counters[kCounterThree];
+    const int count = queued < a.n ? queued : int(a.n);
+    unsigned long long evals = 0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+    {
+        const unsigned long long task = a.threes[k];
+        const int64_t i = int64_t(task >> 1);
+        if (i < 0 || i >= a.n || !(task & 1u))
+            continue;
+        DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+        Driver<NC> d;
+        d.st = &states[i];
+        d.s.setup(&F, d.st->sal);
+        d.s.err = d.st->err;
+        Result<NC> full = d.st->lastPhysical;
+        if (d.s.err || d.recoveryOneAccept(full))
         {
             if (d.s.err)
             {
@@ -828,6 +992,7 @@ size_t stagedScratchBytes(int64_t n, const FluidDev &F)
     add(sizeof(int) * size_t(n));
     add(sizeof(int) * size_t(n));
     add(sizeof(int) * kCounterWords);
+    add(sizeof(unsigned long long) * size_t(n));
     const int64_t cap = contCapacity(n);
     add(sizeof(int) * size_t(cap));
     add(sizeof(AnchorOut<NC>) * size_t(cap) * kAnchors);
@@ -857,6 +1022,7 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
     a.split[0] = reinterpret_cast<int *>(take(sizeof(int) * size_t(n)));
     a.split[1] = reinterpret_cast<int *>(take(sizeof(int) * size_t(n)));
     a.counters = reinterpret_cast<int *>(take(sizeof(int) * kCounterWords));
+    a.threes = reinterpret_cast<unsigned long long *>(take(sizeof(unsigned long long) * size_t(n)));
     a.contCap = contCapacity(n);
     a.cont = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.contCap)));
     a.anchors = take(sizeof(AnchorOut<NC>) * size_t(a.contCap) * kAnchors);
@@ -903,12 +1069,16 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         stagedClassifyKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, round);
         stagedResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round, 0);
         stagedResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round, 1);
+        stagedThreeKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a);
+        stagedThreeResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round);
         stagedResetSplitKernel<<<1, 1, 0, st>>>(a.counters);
         if (after("resume", round + 1))
             return setError(NZ_ERR_CUDA, "staged flash self-check failed in resume");
     }
     stagedRr3MemoKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
     stagedRecoverStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
+    stagedThreeKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a);
+    stagedRecoverThreeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     if (after("recover", kMaxRounds))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
     for (int rr = 0; rr < kRecoveryRounds; ++rr)
