@@ -13,7 +13,13 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
 {
     const int64_t n = a.g.ncell;
     const unsigned grid = unsigned((n + kNatBlock - 1) / kNatBlock);
-    const unsigned warpGrid = unsigned((n * 32 + kNatBlock - 1) / kNatBlock);   // one warp per cell
+    // Phase-state solves: a warp per cell while the cells cannot fill the GPU
+    // with threads, a thread per cell beyond that.
+    int device = 0, smCount = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
+    const int width = n >= int64_t(smCount) * 256 ? 1 : 32;
+    const unsigned warpGrid = unsigned((n * width + kNatBlock - 1) / kNatBlock);
     switch (op)
     {
     case NAT_CACHE:
@@ -36,11 +42,11 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
         break;
     case NAT_UPDATE:
         natUpdateKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.primary, a.ps, a.newPrimary, a.newPs,
-                                                       a.status, a.firstFailure);
+                                                           a.status, a.firstFailure, width);
         break;
     case NAT_INIT:
         natInitKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
-                                                     a.firstFailure);
+                                                         a.firstFailure, width);
         break;
     default:
         return setError(NZ_ERR_ARGUMENT, "natLaunch: unknown operation %d", op);

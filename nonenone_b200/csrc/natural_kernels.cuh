@@ -355,19 +355,22 @@ __global__ void __launch_bounds__(kNatBlock) natHistoryKernel(const __grid_const
         atomicOr(flag, 1);
 }
 
-// One warp per cell: the lanes split the seeds of the cell's stability tests.
+// Width 32: one warp per cell, the lanes splitting the seeds of the cell's
+// stability tests (short latency, for grids too small to fill the GPU).
+// Width 1: one thread per cell (a warp's lanes hold 32 cells, so the solver's
+// per-lane stack is shared by 32 times fewer cells in flight).
 template <int NC>
 __global__ void __launch_bounds__(kNatBlock) natUpdateKernel(const __grid_constant__ FluidDev F,
                                                              const __grid_constant__ NatConst K, int64_t ncell,
                                                              const double *primary, const double *ps,
                                                              double *newPrimary, double *newPs, uint8_t *status,
-                                                             unsigned long long *firstFailure)
+                                                             unsigned long long *firstFailure, int width)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = width == 32 ? int(threadIdx.x & 31) : 0;
+    const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / width;
     if (c >= ncell)
         return;
-    const uint8_t s = cellUpdate<NC>(F, K, primary, ps, c, newPrimary, newPs, lane, 32);
+    const uint8_t s = cellUpdate<NC>(F, K, primary, ps, c, newPrimary, newPs, lane, width);
     if (lane != 0)
         return;
     status[c] = s;
@@ -375,18 +378,18 @@ __global__ void __launch_bounds__(kNatBlock) natUpdateKernel(const __grid_consta
         atomicMin(firstFailure, (unsigned long long)c);
 }
 
-// One warp per cell, as the update.
+// Width 32 or 1, as the update.
 template <int NC>
 __global__ void __launch_bounds__(kNatBlock) natInitKernel(const __grid_constant__ FluidDev F,
                                                            const __grid_constant__ NatConst K, int64_t ncell,
                                                            const double *P, const double *z, double *primary,
-                                                           double *ps, unsigned long long *firstFailure)
+                                                           double *ps, unsigned long long *firstFailure, int width)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = width == 32 ? int(threadIdx.x & 31) : 0;
+    const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / width;
     if (c >= ncell)
         return;
-    if (!cellInitPtz<NC>(F, K, P, z, c, primary, ps, lane, 32) && lane == 0)
+    if (!cellInitPtz<NC>(F, K, P, z, c, primary, ps, lane, width) && lane == 0)
         atomicMin(firstFailure, (unsigned long long)c);
 }
 #endif

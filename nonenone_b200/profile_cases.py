@@ -1,0 +1,85 @@
+"""Single workloads to run under a profiler (one process, one GPU).
+
+  python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged]
+      one N-point batch of the seeded flash mixture (after a 4,096-point warm-up
+      batch, so kernels of the measured batch come second)
+  python -m nonenone_b200.profile_cases natural NX NY NZ
+      P-T-z initialisation of an NX x NY x NZ grid of the H2O/CO2/nC10 case,
+      then two residual + Jacobian evaluations of the accepted state
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+import numpy as np
+
+
+def run_flash(n: int, precision: str) -> None:
+    import torch
+    from . import abi, synth
+    from .flash import CubicThreePhaseFlash
+    from .fluids import make_fluid
+    prec = abi.PRECISION_FP64 if precision == "fp64" else abi.PRECISION_FP64_STAGED
+    fl = CubicThreePhaseFlash(make_fluid())
+    P, T, z = synth.flash_points(n, seed=1)
+    fl.flash(P[:4096], T[:4096], np.ascontiguousarray(z[:, :4096]), precision=prec)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dP, dT, dz = (torch.as_tensor(x, device=fl.device) for x in (P, T, z))
+    out = fl.allocate(n)
+    a.record()
+    fl.flash(dP, dT, dz, precision=prec, out=out)
+    b.record()
+    torch.cuda.synchronize()
+    print(f"flash {n} points: {a.elapsed_time(b):.1f} ms, status counts "
+          f"{np.bincount(out['status'].cpu().numpy(), minlength=5).tolist()}, "
+          f"{fl.eos_eval_count()} EOS evaluations")
+
+
+def run_natural(nx: int, ny: int, nz: int) -> None:
+    import torch
+    from . import abi, synth
+    from .flash import Context, CubicThreePhaseFlash
+    from .fluids import make_fluid
+    from .natural import NaturalAssembler
+    grid, P, z = synth.natural_case(0, nx=nx, ny=ny, nz=nz)
+    fluid = make_fluid()
+    ctx = Context(fluid)
+    nat = NaturalAssembler(ctx, grid, 864.0, 353.15, abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10))
+    fl = CubicThreePhaseFlash(fluid)
+    st = fl.flash(P, np.full(grid.ncell, 353.15), np.ascontiguousarray(z.T),
+                  precision=abi.PRECISION_FP64_STAGED)["status"].cpu().numpy()
+    bad, good = np.where(st != 0)[0], np.where(st == 0)[0]
+    P[bad], z[bad] = P[good[:bad.size]], z[good[:bad.size]]
+    primary, ps = nat.initialize_from_ptz(P, z)
+    nat.refresh_history(primary, ps)
+    vals = torch.empty(nat.nnzb, nat.B, nat.B, dtype=torch.float64, device=primary.device)
+    F = torch.empty_like(primary)
+    for _ in range(2):
+        nat.form_function(primary, ps, out=F)
+        nat.assemble_jacobian(primary, ps, values=vals)
+    torch.cuda.synchronize()
+    print(f"natural {nx}x{ny}x{nz}: {grid.ncell} cells, {nat.nnzb} blocks, "
+          f"{vals.numel() * 8 / 1e9:.3f} GB of Jacobian values")
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="case", required=True)
+    f = sub.add_parser("flash")
+    f.add_argument("n", type=int)
+    f.add_argument("--precision", default="fp64_staged", choices=["fp64", "fp64_staged"])
+    nat = sub.add_parser("natural")
+    nat.add_argument("nx", type=int)
+    nat.add_argument("ny", type=int)
+    nat.add_argument("nz", type=int)
+    a = ap.parse_args(argv)
+    if a.case == "flash":
+        run_flash(a.n, a.precision)
+    else:
+        run_natural(a.nx, a.ny, a.nz)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
