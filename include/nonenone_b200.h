@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define NZ_ABI_VERSION 1
+#define NZ_ABI_VERSION 2
 #define NZ_MAX_NC 8
 
 /* ---- status codes ------------------------------------------------------ */
@@ -62,6 +62,13 @@ extern "C" {
 #define NZ_EOS_SW 1
 #define NZ_EOS_CPA 2
 
+/* CPA cubic term and radial distribution (thermodynamic_model.hpp:19-23,
+ * cubic_plus_association.hpp:19-23) */
+#define NZ_CPA_SRK 0
+#define NZ_CPA_PR 1
+#define NZ_CPA_RADIAL_SIMPLIFIED 0
+#define NZ_CPA_RADIAL_CARNAHAN_STARLING 1
+
 /* SW aqueous H2O-solute BIP correlation per component (cubic_eos.hpp:2389-2404) */
 #define NZ_SW_BIP_KIJ 0            /* keep the ordinary k_ij */
 #define NZ_SW_BIP_CONSTANT 1       /* sw_bip_value[c] */
@@ -86,6 +93,27 @@ typedef struct nz_fluid_desc {
     double sw_salinity;         /* NaCl molality used when no per-point salinity */
     int32_t sw_bip_kind[NZ_MAX_NC];
     double sw_bip_value[NZ_MAX_NC];
+    /* PR-CPA / SRK-CPA (eos_model = NZ_EOS_CPA): CubicEquationOfState::
+     * CubicPlusAssociationOptions (models/include/natural/thermo/cubic_eos.hpp:117-136).
+     * The flash and EOS entry points carry one associating component with equal
+     * donor and acceptor sites, or one donor-bearing component with any acceptors
+     * (e.g. 4C water with CO2 as an acceptor); fluids with several donor-bearing
+     * components give NZ_FLASH_NOT_PORTED per point.  The Natural entry points
+     * refuse CPA. */
+    double cpa_a0[NZ_MAX_NC];            /* Pa m6/mol2 */
+    double cpa_b[NZ_MAX_NC];             /* m3/mol */
+    double cpa_c1[NZ_MAX_NC];
+    double cpa_epsilon[NZ_MAX_NC];       /* association energy, J/mol */
+    double cpa_beta[NZ_MAX_NC];          /* association volume */
+    int32_t cpa_donor_sites[NZ_MAX_NC];
+    int32_t cpa_acceptor_sites[NZ_MAX_NC];
+    double cpa_cross_epsilon[NZ_MAX_NC * NZ_MAX_NC];  /* [donor][acceptor]; positive */
+    double cpa_cross_beta[NZ_MAX_NC * NZ_MAX_NC];     /* entries override the CR-1 rule */
+    int32_t cpa_physical_term;           /* NZ_CPA_SRK or NZ_CPA_PR */
+    int32_t cpa_radial;                  /* NZ_CPA_RADIAL_SIMPLIFIED or _CARNAHAN_STARLING */
+    int32_t cpa_max_association_iterations;  /* 2000 */
+    double cpa_association_tolerance;    /* 1e-12 */
+    double cpa_association_damping;      /* 0.2 */
 } nz_fluid_desc;
 
 /* ThreePhaseFlashOptions (three_phase_flash_types.hpp:21-41) */

@@ -16,6 +16,8 @@ NZ_ERR_CUDA = -2
 NZ_ERR_UNSUPPORTED = -3
 
 EOS_PR, EOS_SW, EOS_CPA = 0, 1, 2
+CPA_SRK, CPA_PR = 0, 1
+CPA_RADIAL_SIMPLIFIED, CPA_RADIAL_CARNAHAN_STARLING = 0, 1
 SW_BIP_KIJ, SW_BIP_CONSTANT, SW_BIP_CO2, SW_BIP_HYDROCARBON, SW_BIP_CO2_CHABAB = range(5)
 
 FLASH_CONVERGED, FLASH_FAILED, FLASH_BAD_INPUT, FLASH_EOS_ERROR, FLASH_NOT_PORTED = range(5)
@@ -47,6 +49,20 @@ class FluidDesc(C.Structure):
         ("sw_salinity", C.c_double),
         ("sw_bip_kind", C.c_int32 * MAX_NC),
         ("sw_bip_value", C.c_double * MAX_NC),
+        ("cpa_a0", C.c_double * MAX_NC),
+        ("cpa_b", C.c_double * MAX_NC),
+        ("cpa_c1", C.c_double * MAX_NC),
+        ("cpa_epsilon", C.c_double * MAX_NC),
+        ("cpa_beta", C.c_double * MAX_NC),
+        ("cpa_donor_sites", C.c_int32 * MAX_NC),
+        ("cpa_acceptor_sites", C.c_int32 * MAX_NC),
+        ("cpa_cross_epsilon", C.c_double * (MAX_NC * MAX_NC)),
+        ("cpa_cross_beta", C.c_double * (MAX_NC * MAX_NC)),
+        ("cpa_physical_term", C.c_int32),
+        ("cpa_radial", C.c_int32),
+        ("cpa_max_association_iterations", C.c_int32),
+        ("cpa_association_tolerance", C.c_double),
+        ("cpa_association_damping", C.c_double),
     ]
 
 

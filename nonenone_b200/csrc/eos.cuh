@@ -67,6 +67,7 @@ constexpr uint8_t OIL_BIT = 1, GAS_BIT = 2, WATER_BIT = 4, ALL_BITS = 7;
 
 constexpr int EOS_PR = 0;
 constexpr int EOS_SW = 1;
+constexpr int EOS_CPA = 2;
 
 // Error codes a thread can raise where the reference throws.
 constexpr int ERR_NONE = 0;
@@ -115,6 +116,23 @@ struct FlashOpts
     double fdStep;
 };
 
+// Cubic-plus-association parameters (CubicEquationOfState::CubicPlusAssociationOptions,
+// cubic_eos.hpp:117-136), with the association scheme classified once on the host.
+struct CpaDev
+{
+    double a0[kMaxNc], b[kMaxNc], c1[kMaxNc];
+    double epsilon[kMaxNc], beta[kMaxNc];
+    int donor[kMaxNc], acceptor[kMaxNc];
+    double crossEpsilon[kMaxNc * kMaxNc], crossBeta[kMaxNc * kMaxNc];
+    int pengRobinson;        // physical term: 1 Peng-Robinson, 0 Soave-Redlich-Kwong
+    int carnahanStarling;    // radial distribution: 1 Carnahan-Starling, 0 simplified
+    int maxIterations;
+    double tolerance;
+    double damping;
+    int symmetric;           // the only associating component, with equal donor/acceptor sites, else -1
+    int singleDonor;         // the only donor-bearing component, else -1
+};
+
 // Fluid constants as kernels see them (by value, __grid_constant__).
 struct FluidDev
 {
@@ -130,6 +148,7 @@ struct FluidDev
     int swKind[kMaxNc];
     double swValue[kMaxNc];
     FlashOpts opt;
+    CpaDev cpa;
 };
 
 template <int NC>

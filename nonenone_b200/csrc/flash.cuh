@@ -19,6 +19,7 @@
 #pragma once
 
 #include "eos.cuh"
+#include "cpa.cuh"
 
 namespace nz
 {
@@ -292,6 +293,22 @@ struct Solver
     // phaseResultForThermodynamicRole_ (core.inc:101-126)
     NZ_HDN double phaseForRole(int role, double P, double T, const double *x, double *phi)
     {
+        if (F->eosModel == EOS_CPA)
+        {
+            // phaseResult's CPA branch (core.inc:108-112 -> cubic_eos.hpp:842-846)
+            ++evals;
+            double Z = 0.0;
+            const int rc = cpaPhase<NC>(*F, P, T, x, role != GAS, Z, phi);
+            if (rc != ERR_NONE)
+            {
+                fail(rc);
+                const double nan = nzNan();
+                for (int i = 0; i < NC; ++i)
+                    phi[i] = nan;
+                return nan;
+            }
+            return Z;
+        }
         ensureCache(P, T);
         const MixParams<NC> &p = (role == WATER && sw()) ? aq : nonAq;
         PhaseMix<NC> m;

@@ -79,8 +79,20 @@ eosKernel(const __grid_constant__ FluidDev F, int64_t n, const double *__restric
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    MixParams<NC> p;
     const int r = role[i];
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    if (F.eosModel == EOS_CPA)
+    {
+        double xc[NC], phi[NC], Z = 0.0;
+        for (int c = 0; c < NC; ++c)
+            xc[c] = x[c * n + i];
+        const bool ok = cpaPhase<NC>(F, P[i], T[i], xc, r != GAS, Z, phi) == ERR_NONE;
+        Zout[i] = ok ? Z : nan;
+        for (int c = 0; c < NC; ++c)
+            lnphi[c * n + i] = ok ? log(phi[c]) : nan;
+        return;
+    }
+    MixParams<NC> p;
     mixingParameters<NC>(F, P[i], T[i], salinity ? salinity[i] : F.salinity, r == WATER, p);
     double xi[NC];
 #pragma unroll
@@ -91,7 +103,6 @@ eosKernel(const __grid_constant__ FluidDev F, int64_t n, const double *__restric
     const double Z = selectCubicRoot(m.A, m.B, F.m1, F.m2, r == GAS);
     double phi[NC];
     const bool ok = isfinite(Z) && fugacityCoefficients<NC>(xi, p, m, Z, F.m1, F.m2, phi);
-    const double nan = __longlong_as_double(0x7ff8000000000000LL);
     Zout[i] = ok ? Z : nan;
 #pragma unroll
     for (int c = 0; c < NC; ++c)

@@ -52,6 +52,51 @@ FluidDev makeFluidDev(const nz_fluid_desc &d, const nz_flash_options &o)
     for (int k = 0; k < kMaxNc * kMaxNc; ++k)
         f.kij[k] = d.kij[k];
     f.salinity = d.sw_salinity;
+    // CPA parameters and the association scheme (cpaWaterOnlyAnalyticFastPathAvailable_,
+    // cpaSingleSymmetricAssociatingComponent_, cpaSingleDonorComponent_; cubic_eos.hpp:1305-1354)
+    CpaDev &c = f.cpa;
+    for (int i = 0; i < kMaxNc; ++i)
+    {
+        c.a0[i] = d.cpa_a0[i];
+        c.b[i] = d.cpa_b[i];
+        c.c1[i] = d.cpa_c1[i];
+        c.epsilon[i] = d.cpa_epsilon[i];
+        c.beta[i] = d.cpa_beta[i];
+        c.donor[i] = i < d.nc ? d.cpa_donor_sites[i] : 0;
+        c.acceptor[i] = i < d.nc ? d.cpa_acceptor_sites[i] : 0;
+    }
+    for (int k = 0; k < kMaxNc * kMaxNc; ++k)
+    {
+        c.crossEpsilon[k] = d.cpa_cross_epsilon[k];
+        c.crossBeta[k] = d.cpa_cross_beta[k];
+    }
+    c.pengRobinson = d.cpa_physical_term == NZ_CPA_PR ? 1 : 0;
+    c.carnahanStarling = d.cpa_radial == NZ_CPA_RADIAL_CARNAHAN_STARLING ? 1 : 0;
+    c.maxIterations = d.cpa_max_association_iterations;
+    c.tolerance = d.cpa_association_tolerance;
+    c.damping = d.cpa_association_damping;
+    c.symmetric = -1;
+    c.singleDonor = -1;
+    int associating = -1, donors = 0, donorComponent = -1;
+    bool symmetricOk = true;
+    for (int i = 0; i < d.nc; ++i)
+    {
+        const int dn = c.donor[i], ac = c.acceptor[i];
+        if (dn > 0)
+        {
+            ++donors;
+            donorComponent = i;
+        }
+        if (dn == 0 && ac == 0)
+            continue;
+        if (associating >= 0 || dn <= 0 || dn != ac)
+            symmetricOk = false;
+        associating = i;
+    }
+    if (symmetricOk && associating >= 0)
+        c.symmetric = associating;
+    else if (donors == 1)
+        c.singleDonor = donorComponent;
     f.opt.maxIterations = o.maximum_iterations;
     f.opt.maxRr = o.maximum_rachford_rice_iterations;
     f.opt.maxStability = o.maximum_stability_iterations;
@@ -124,8 +169,16 @@ int nz_ctx_create(const nz_fluid_desc *fluid, const nz_flash_options *options, i
     *out = nullptr;
     if (!ncSupported(fluid->nc))
         return setError(NZ_ERR_UNSUPPORTED, "nz_ctx_create: nc=%d not compiled (3,4,5,6,8)", fluid->nc);
-    if (fluid->eos_model != NZ_EOS_PR && fluid->eos_model != NZ_EOS_SW)
-        return setError(NZ_ERR_UNSUPPORTED, "nz_ctx_create: only PR and SW EOS are carried");
+    if (fluid->eos_model != NZ_EOS_PR && fluid->eos_model != NZ_EOS_SW && fluid->eos_model != NZ_EOS_CPA)
+        return setError(NZ_ERR_UNSUPPORTED, "nz_ctx_create: unknown eos_model %d", fluid->eos_model);
+    if (fluid->eos_model == NZ_EOS_CPA)
+    {
+        if (fluid->cpa_max_association_iterations <= 0 || !(fluid->cpa_association_tolerance > 0.0))
+            return setError(NZ_ERR_ARGUMENT, "nz_ctx_create: CPA association iterations and tolerance must be positive");
+        for (int i = 0; i < fluid->nc; ++i)
+            if (!(fluid->cpa_b[i] > 0.0) || fluid->cpa_donor_sites[i] < 0 || fluid->cpa_acceptor_sites[i] < 0)
+                return setError(NZ_ERR_ARGUMENT, "nz_ctx_create: CPA co-volume / site counts of component %d", i);
+    }
     if (fluid->eos_type != 1 && fluid->eos_type != 5)
         return setError(NZ_ERR_ARGUMENT, "nz_ctx_create: eos_type must be 1 or 5");
     if (fluid->water_component < -1 || fluid->water_component >= fluid->nc)

@@ -246,6 +246,8 @@ int nz_natural_create(nz_ctx *ctx, const nz_natural_desc *desc, nz_natural **out
     *out = nullptr;
     if (!ctx || !desc)
         return setError(NZ_ERR_ARGUMENT, "nz_natural_create: null argument");
+    if (ctx->fluid.eosModel == nz::EOS_CPA)
+        return setError(NZ_ERR_UNSUPPORTED, "nz_natural_create: the Natural kernels carry PR and SW, not CPA");
     if (ctx->fluid.water < 0)
         return setError(NZ_ERR_ARGUMENT, "nz_natural_create: the fully compositional model needs a water component");
     const nz_natural_desc &d = *desc;

@@ -18,8 +18,8 @@ from __future__ import annotations
 
 import math
 
-from .abi import (EOS_PR, EOS_SW, FluidDesc, MAX_NC, SW_BIP_CO2,
-                  SW_BIP_HYDROCARBON, SW_BIP_KIJ)
+from .abi import (CPA_PR, CPA_RADIAL_SIMPLIFIED, EOS_CPA, EOS_PR, EOS_SW, FluidDesc, MAX_NC,
+                  SW_BIP_CO2, SW_BIP_HYDROCARBON, SW_BIP_KIJ)
 
 OMEGA_A = 0.4572355
 OMEGA_B = 0.0779691
@@ -84,4 +84,71 @@ def make_fluid(names=H2O_CO2_NC10, eos_model: int = EOS_PR, eos_type: int = 1,
             d.sw_bip_kind[i] = SW_BIP_CO2 if n == "CO2" else SW_BIP_HYDROCARBON
         else:
             d.sw_bip_kind[i] = SW_BIP_KIJ
+    return d
+
+
+GAS_CONSTANT = 8.31446261815324
+
+# Standard 4C water of SRK-CPA (models/include/natural/thermo/cubic_plus_association.hpp:31-40)
+WATER_4C = dict(a0=0.12277, b=1.4515e-5, c1=0.67359, epsilon=16655.0, beta=0.0692, donor=2, acceptor=2)
+
+
+def set_cpa(d: FluidDesc, names, physical_term: int = CPA_PR, water: dict | None = None,
+            radial: int = CPA_RADIAL_SIMPLIFIED) -> FluidDesc:
+    """Make `d` a CPA fluid with the reference factory's defaults
+    (case/include/case/fluid_factory.hpp:323-396): every component's cubic part
+    from Tc, Pc, omega (PR or SRK form; PR78 c1 for omega > 0.49 when eos_type is
+    5), water replaced by the 4C parameter set (or `water`)."""
+    R = GAS_CONSTANT
+    d.eos_model = EOS_CPA
+    d.cpa_physical_term = physical_term
+    d.cpa_radial = radial
+    d.cpa_max_association_iterations = 2000
+    d.cpa_association_tolerance = 1.0e-12
+    d.cpa_association_damping = 0.2
+    for i, n in enumerate(names):
+        tc, pc, _, om, _ = COMPONENTS[n]
+        if physical_term == CPA_PR:
+            d.cpa_a0[i] = 0.45724 * R * R * tc * tc / pc
+            d.cpa_b[i] = 0.07780 * R * tc / pc
+            d.cpa_c1[i] = 0.37464 + 1.54226 * om - 0.26992 * om * om
+            if d.eos_type == 5 and om > 0.49:
+                d.cpa_c1[i] = 0.379642 + 1.48503 * om - 0.164423 * om * om + 0.016666 * om * om * om
+        else:
+            d.cpa_a0[i] = 0.42748 * R * R * tc * tc / pc
+            d.cpa_b[i] = 0.08664 * R * tc / pc
+            d.cpa_c1[i] = 0.480 + 1.574 * om - 0.176 * om * om
+    if "H2O" in names:
+        w = names.index("H2O")
+        p = WATER_4C if water is None else water
+        d.cpa_a0[w], d.cpa_b[w], d.cpa_c1[w] = p["a0"], p["b"], p["c1"]
+        d.cpa_epsilon[w], d.cpa_beta[w] = p["epsilon"], p["beta"]
+        d.cpa_donor_sites[w], d.cpa_acceptor_sites[w] = p["donor"], p["acceptor"]
+    return d
+
+
+def make_cpa_h2o_co2_nc10(co2_acceptor: bool = True) -> FluidDesc:
+    """The PR-CPA H2O/CO2/nC10 fluid of the reference's 60x20 case
+    (case/h2o_co2_nc10_2d_benchmark/case_config.hpp:106-142): water
+    a0 = 0.15782, b = 1.4788e-5, c1 = 0.6736, epsilon = 16123 J/mol,
+    beta = 0.069662 with two donor and two acceptor sites; CO2 one acceptor site
+    cross-associating with water (epsilon 8061.5, beta 0.15182); PR78 c1 for nC10;
+    the case's CPA BIPs (H2O-CO2 0.10566, CO2-nC10 0.1141).  Tc, Pc, omega are the
+    benchmark set of this module.  `co2_acceptor=False` leaves water the only
+    associating component (the analytic site-fraction path)."""
+    names = H2O_CO2_NC10
+    d = make_fluid(names, eos_type=5)
+    for i in range(MAX_NC * MAX_NC):
+        d.kij[i] = 0.0
+    for (a, b), k in (((0, 1), 0.10566), ((1, 2), 0.1141)):
+        d.kij[a * MAX_NC + b] = d.kij[b * MAX_NC + a] = k
+    set_cpa(d, names, CPA_PR, water=dict(a0=0.15782, b=1.4788e-5, c1=0.6736, epsilon=16123.0,
+                                         beta=0.069662, donor=2, acceptor=2))
+    tc, pc, _, om, _ = COMPONENTS["nC10"]
+    d.cpa_c1[2] = 0.379642 + 1.48503 * om - 0.164423 * om * om + 0.016666 * om * om * om
+    if co2_acceptor:
+        d.cpa_epsilon[1], d.cpa_beta[1] = 8061.5, 0.15182
+        d.cpa_acceptor_sites[1] = 1
+        d.cpa_cross_epsilon[0 * MAX_NC + 1] = 8061.5
+        d.cpa_cross_beta[0 * MAX_NC + 1] = 0.15182
     return d

@@ -60,7 +60,7 @@ def load():
         L.nz_jacobian.argtypes = [vp, vp, vp, vp, vp, vp]
     L.nz_diag_fma_peak.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.nz_flash_batch_noalloc.argtypes = [vp, i64, vp, vp, vp, vp, vp, i32, vp]
-    if L.nz_abi_version() != 1:
+    if L.nz_abi_version() != 2:
         raise NzError("ABI version mismatch")
     _lib = L
     return _lib

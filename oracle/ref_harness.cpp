@@ -108,9 +108,39 @@ CubicEquationOfState<Indices> makeEos(const nz_fluid_desc &d, double salinity)
         }
         eos.configureSoreideWhitson(std::move(sw));
     }
+    else if (d.eos_model == NZ_EOS_CPA)
+    {
+        // CubicPlusAssociationOptions filled as case/include/case/fluid_factory.hpp:323-396 does
+        typename CubicEquationOfState<Indices>::CubicPlusAssociationOptions cpa;
+        for (int c = 0; c < N; ++c)
+        {
+            const auto cc = static_cast<std::size_t>(c);
+            cpa.a0[cc] = d.cpa_a0[c];
+            cpa.b[cc] = d.cpa_b[c];
+            cpa.c1[cc] = d.cpa_c1[c];
+            cpa.associationEnergy[cc] = d.cpa_epsilon[c];
+            cpa.associationVolume[cc] = d.cpa_beta[c];
+            cpa.donorSites[cc] = d.cpa_donor_sites[c];
+            cpa.acceptorSites[cc] = d.cpa_acceptor_sites[c];
+            for (int j = 0; j < N; ++j)
+            {
+                cpa.crossAssociationEnergy[cc][static_cast<std::size_t>(j)] = d.cpa_cross_epsilon[c * NZ_MAX_NC + j];
+                cpa.crossAssociationVolume[cc][static_cast<std::size_t>(j)] = d.cpa_cross_beta[c * NZ_MAX_NC + j];
+            }
+        }
+        cpa.physicalTerm = d.cpa_physical_term == NZ_CPA_PR ? CpaCubicPhysicalTerm::PengRobinson
+                                                            : CpaCubicPhysicalTerm::SoaveRedlichKwong;
+        cpa.radialDistribution = d.cpa_radial == NZ_CPA_RADIAL_CARNAHAN_STARLING
+            ? CpaRadialDistribution::CarnahanStarling
+            : CpaRadialDistribution::Simplified;
+        cpa.maximumAssociationIterations = d.cpa_max_association_iterations;
+        cpa.associationTolerance = d.cpa_association_tolerance;
+        cpa.associationDamping = d.cpa_association_damping;
+        eos.configureCubicPlusAssociation(std::move(cpa));
+    }
     else if (d.eos_model != NZ_EOS_PR)
     {
-        throw std::invalid_argument("oracle: only PR and SW are wired");
+        throw std::invalid_argument("oracle: unknown eos_model");
     }
     return eos;
 }
@@ -663,6 +693,7 @@ int dispatchNc(int nc, Args &&...args)
 {
     switch (nc)
     {
+    case 2: return F<2>::run(std::forward<Args>(args)...);
     case 3: return F<3>::run(std::forward<Args>(args)...);
     case 4: return F<4>::run(std::forward<Args>(args)...);
     case 5: return F<5>::run(std::forward<Args>(args)...);

@@ -8,6 +8,8 @@ reference's own FP64 C++ (oracle/_ref/libnzref.so); the inputs are seeded
   flash_pr_nc3.npz  2048 points of the batched-flash mixture, PR
   flash_sw_nc3.npz  1024 points, Soreide-Whitson, salinity ~ U[0,2]
   flash_pr_nc6.npz  512 points, six components, PR
+  flash_cpa_nc3.npz 1024 points, PR-CPA H2O/CO2/nC10 of the reference's 60x20 case
+                    (4C water, CO2 one acceptor site: the single-donor path)
   flash_continuation_pr_nc3.npz  192 points of the 1,048,576-point bench batch
                     (synth.flash_points(2**20, seed=1)) that reach the flash's last
                     fallback, the pressure continuation: 160 it rescues and 32 it
@@ -30,7 +32,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from nonenone_b200 import abi, synth  # noqa: E402
-from nonenone_b200.fluids import SIX_COMPONENT, make_fluid  # noqa: E402
+from nonenone_b200.fluids import SIX_COMPONENT, make_cpa_h2o_co2_nc10, make_fluid  # noqa: E402
 from oracle import ref  # noqa: E402
 
 
@@ -103,6 +105,8 @@ def main():
     T = rng.uniform(303.0, 423.0, n)
     z = np.ascontiguousarray(rng.dirichlet([4, 2, 1, 1, 1, 1], n).T)
     make("flash_pr_nc6.npz", six, P, T, z)
+    P, T, z = synth.flash_points(1024, seed=104)
+    make("flash_cpa_nc3.npz", make_cpa_h2o_co2_nc10(), P, T, z)
     P, T, z = synth.flash_points(1 << 20, seed=1)
     sel = np.array(RESCUED + FAILING)
     make("flash_continuation_pr_nc3.npz", pr, P[sel], T[sel], np.ascontiguousarray(z[:, sel]))

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
     lib = C.CDLL(LIB_PATH)
     missing = [s for s in declared_functions() if not hasattr(lib, s)]
     assert not missing, missing
-    assert lib.nz_abi_version() == 1
+    assert lib.nz_abi_version() == 2
 
 
 def test_struct_layouts_match_c(tmp_path):

@@ -9,8 +9,8 @@ Tolerances (from the benchmark definition):
 import numpy as np
 import pytest
 
-from nonenone_b200 import abi
-from nonenone_b200.fluids import SIX_COMPONENT, make_fluid
+from nonenone_b200 import abi, synth
+from nonenone_b200.fluids import SIX_COMPONENT, make_cpa_h2o_co2_nc10, make_fluid
 from tests import kat
 
 pytestmark = pytest.mark.gpu
@@ -63,6 +63,12 @@ def compare_flash(gpu, g, max_boundary_fraction=0.02):
         err = np.abs(a - b) / np.maximum(1.0, np.abs(b))
         assert err.max() <= 1e-7, (key, err.max())
     return int(mism.sum())
+
+
+def _fluid(args):
+    if args.get("cpa"):
+        return make_cpa_h2o_co2_nc10()
+    return make_fluid(**args)
 
 
 def test_eos_kat_on_gpu(torch_cuda):
@@ -119,11 +125,12 @@ def test_flash_three_phase_kat_on_gpu(torch_cuda):
     ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
     ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
     ("flash_continuation_pr_nc3.npz", dict()),
+    ("flash_cpa_nc3.npz", dict(cpa=True)),
 ])
 def test_flash_matches_golden(torch_cuda, golden, name, fluid_args):
     from nonenone_b200.flash import CubicThreePhaseFlash
     g = golden(name)
-    fl = CubicThreePhaseFlash(make_fluid(**fluid_args))
+    fl = CubicThreePhaseFlash(_fluid(fluid_args))
     out = _np(fl.flash(g["P"], g["T"], g["z"], salinity=g.get("salinity")))
     compare_flash(out, g)
 
@@ -192,12 +199,13 @@ def test_stability_matches_reference(torch_cuda, reference, golden):
     ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
     ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
     ("flash_continuation_pr_nc3.npz", dict()),
+    ("flash_cpa_nc3.npz", dict(cpa=True)),
 ])
 def test_staged_fp64_matches_golden(torch_cuda, golden, name, fluid_args):
     """The staged FP64 form (driver / trial kernels) against the reference."""
     from nonenone_b200.flash import CubicThreePhaseFlash
     g = golden(name)
-    fl = CubicThreePhaseFlash(make_fluid(**fluid_args))
+    fl = CubicThreePhaseFlash(_fluid(fluid_args))
     out = _np(fl.flash(g["P"], g["T"], g["z"], salinity=g.get("salinity"),
                        precision=abi.PRECISION_FP64_STAGED))
     compare_flash(out, g)
@@ -213,3 +221,36 @@ def test_staged_fp64_equals_plain_fp64(torch_cuda, golden):
     assert np.array_equal(a["status"], b["status"]) and np.array_equal(a["presence"], b["presence"])
     ok = a["status"] == 0
     assert np.abs(a["beta"][:, ok] - b["beta"][:, ok]).max() < 1e-13
+
+
+@pytest.mark.parametrize("co2_acceptor", [True, False])
+def test_cpa_eos_matches_reference_random(torch_cuda, reference, co2_acceptor):
+    """PR-CPA phase evaluations: the single-donor path (4C water + CO2 acceptor)
+    and the analytic path (water the only associating component)."""
+    from nonenone_b200.flash import CubicEquationOfState
+    f = make_cpa_h2o_co2_nc10(co2_acceptor)
+    rng = np.random.default_rng(8)
+    n = 3000
+    P = rng.uniform(1e6, 60e6, n)
+    T = rng.uniform(290, 450, n)
+    x = np.ascontiguousarray(rng.dirichlet([2, 1, 1], n).T)
+    role = rng.integers(0, 3, n).astype(np.int8)
+    Zr, lr = reference.eos_phase_batch(f, P, T, x, role)
+    Zg, lg = CubicEquationOfState(f).phase_result(P, T, x, role)
+    Zg, lg = Zg.cpu().numpy(), lg.cpu().numpy()
+    assert np.array_equal(np.isfinite(Zr), np.isfinite(Zg))
+    m = np.isfinite(Zr)
+    assert kat.near(Zg[m], Zr[m], 1e-11)
+    assert kat.near(lg[:, m], lr[:, m], 1e-10)
+
+
+def test_cpa_with_several_donors_is_reported_not_ported(torch_cuda):
+    """A fluid with two donor-bearing components needs the general association
+    solve, which is not carried: every point says so instead of answering."""
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    f = make_cpa_h2o_co2_nc10()
+    f.cpa_donor_sites[1] = 1
+    P, T, z = synth.flash_points(64, seed=5)
+    for precision in (abi.PRECISION_FP64, abi.PRECISION_FP64_STAGED):
+        out = _np(CubicThreePhaseFlash(f).flash(P, T, z, precision=precision))
+        assert np.all(out["status"] == abi.FLASH_NOT_PORTED)

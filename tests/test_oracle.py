@@ -58,3 +58,26 @@ def test_golden_label_mix(golden):
     single = np.isin(pres, [1, 2, 4]).sum() / n
     three = (pres == 7).sum() / n
     assert 0.33 < single < 0.47 and 0.14 < three < 0.26
+
+
+def test_oracle_cpa_water_methanol_kat(reference):
+    """SRK-CPA water/methanol liquid compressibility recorded by the reference
+    (case/five_component_eos_tuned_compare/RUN_REPORT.md:105, the water_methanol
+    case of test/src/benchmark/cpa_phase_benchmark.cpp): Z = 0.002920191895."""
+    from nonenone_b200.abi import CPA_SRK, EOS_CPA, MAX_NC, FluidDesc
+    d = FluidDesc()
+    d.nc, d.eos_model, d.eos_type, d.water_component = 2, EOS_CPA, 1, 0
+    d.omega_a, d.omega_b, d.m1, d.m2, d.minimum_composition = 0.42748, 0.08664, 1.0, 0.0, 1.0e-30
+    for i, (tc, pc, vc, om, mw) in enumerate(((647.3, 22.0483e6, 5.60e-5, 0.344, 0.018015),
+                                              (512.6, 8.0959e6, 1.18e-4, 0.559, 0.032042))):
+        d.tc[i], d.pc[i], d.vc[i], d.acentric[i], d.mw[i] = tc, pc, vc, om, mw
+    d.kij[0 * MAX_NC + 1] = d.kij[1 * MAX_NC + 0] = -0.09
+    for i, (a0, b, c1, eps, beta, sites) in enumerate(((0.12277, 1.4515e-5, 0.67359, 16655.0, 0.0692, 2),
+                                                       (0.40531, 3.0978e-5, 0.43102, 24591.0, 0.0161, 1))):
+        d.cpa_a0[i], d.cpa_b[i], d.cpa_c1[i] = a0, b, c1
+        d.cpa_epsilon[i], d.cpa_beta[i] = eps, beta
+        d.cpa_donor_sites[i] = d.cpa_acceptor_sites[i] = sites
+    d.cpa_physical_term = CPA_SRK
+    d.cpa_max_association_iterations, d.cpa_association_tolerance, d.cpa_association_damping = 2000, 1e-12, 0.2
+    Z, _ = reference.eos_phase_batch(d, [233183.46666657156], [389.375], [[0.185], [0.815]], [0])
+    assert abs(Z[0] - 0.002920191895) < 5e-13
