@@ -211,8 +211,8 @@ int nz_flash_eos_eval_count(nz_ctx* ctx, uint64_t* count);
  * static device array of NZ_NOALLOC_SCRATCH_BYTES that every GPU which loads
  * this library holds until the process exits; it calls no cudaMalloc /
  * cudaFree.  Batches whose work space would exceed the array are rejected
- * with NZ_ERR_ARGUMENT (at most 14,462 points for nc = 3, 7,947 for nc = 6,
- * 5,855 for nc = 8).  The first call on a
+ * with NZ_ERR_ARGUMENT (at most 14,074 points for nc = 3, 7,742 for nc = 6,
+ * 5,712 for nc = 8).  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress) and
  * should therefore come before any stream capture.  All calls share the one
  * array and the context's evaluation counter: calls that overlap on the GPU
@@ -305,9 +305,15 @@ int nz_natural_init_ptz(nz_natural* nat, const double* P, const double* z,
  * (refreshPreviousPropertiesCache_, natural_petsc_runtime_cache_history.inc:180-262). */
 int nz_natural_set_history(nz_natural* nat, const double* primary,
                            const double* phase_state, void* stream);
-/* Transactional phase-state update of every cell; commits all cells or none. */
+/* Transactional phase-state update of every cell; commits all cells or none.
+ * By default the first stability test of every cell runs on the batched
+ * lane-per-trial kernels (work space held by the nz_natural from its
+ * creation: 2.5 KB per cell for nc = 3, 4.6 KB for nc = 6, 6.2 KB for
+ * nc = 8); results are those of the per-cell tests, which
+ * nz_natural_set_staged_update(nat, 0) selects instead. */
 int nz_update_state(nz_natural* nat, double* primary, double* phase_state,
                     nz_report* report, void* stream);
+int nz_natural_set_staged_update(nz_natural* nat, int32_t enabled);
 /* Residual F[ncell*B] (cell-major). */
 int nz_residual(nz_natural* nat, const double* primary,
                 const double* phase_state, double* residual, void* stream);

@@ -228,6 +228,77 @@ struct Rr3Memo
     }
 };
 
+// A stability test computed ahead of time for one exact input (P, T, z, the
+// active set and its compositions).  stabilityTest returns the stored answer
+// when it is called with identical inputs and tests as usual otherwise.  The
+// batched Natural update uses it to run the main-path test of every cell on
+// the lane-per-trial kernel before the per-cell code runs.
+constexpr uint8_t MEMO_NONE = 0;        // no test recorded
+constexpr uint8_t MEMO_CAPTURED = 1;    // input recorded, answer pending
+constexpr uint8_t MEMO_READY = 2;       // answer stored
+
+template <int NC>
+struct StabilityMemo
+{
+    double P, T;
+    double z[NC];
+    double x[3][NC];
+    StabilityResult<NC> res;
+    int err;
+    uint8_t active;
+    uint8_t state;
+
+    NZ_HD void record(double p, double t, const double *zz, uint8_t act, const double (&xx)[3][NC])
+    {
+        P = p;
+        T = t;
+        active = act;
+        for (int i = 0; i < NC; ++i)
+            z[i] = zz[i];
+        for (int q = 0; q < 3; ++q)
+            for (int i = 0; i < NC; ++i)
+                x[q][i] = xx[q][i];
+        state = MEMO_CAPTURED;
+    }
+
+    NZ_HD bool matches(double p, double t, const double *zz, uint8_t act, const double (&xx)[3][NC]) const
+    {
+        if (state != MEMO_READY || P != p || T != t || active != act)
+            return false;
+        for (int i = 0; i < NC; ++i)
+            if (z[i] != zz[i])
+                return false;
+        for (int q = 0; q < 3; ++q)
+            for (int i = 0; i < NC; ++i)
+                if (x[q][i] != xx[q][i])
+                    return false;
+        return true;
+    }
+};
+
+// A top-level flash computed ahead of time (by the staged batched flash) for
+// one exact input (P, T, z).  flash<true> returns it when called with
+// identical inputs; `err` carries the flash's error code (0 = none).
+template <int NC>
+struct FlashMemo
+{
+    double P, T;
+    double z[NC];
+    Result<NC> r;
+    int err;
+    int valid;
+
+    NZ_HD bool matches(double p, double t, const double *zz) const
+    {
+        if (!valid || P != p || T != t)
+            return false;
+        for (int i = 0; i < NC; ++i)
+            if (z[i] != zz[i])
+                return false;
+        return true;
+    }
+};
+
 // ============================================================================
 template <int NC>
 struct Solver
@@ -249,6 +320,8 @@ struct Solver
     MixParams<NC> nonAq;
     MixParams<NC> aq;
     const Rr3Memo<NC> *memo;   // optional precomputed rr3Robust answer
+    StabilityMemo<NC> *stabMemo;   // optional precomputed stability test
+    const FlashMemo<NC> *flashMemo;   // optional precomputed top-level flash
 
     NZ_HD void setup(const FluidDev *fluid, double s)
     {
@@ -264,6 +337,8 @@ struct Solver
         cacheValid = false;
         cacheP = cacheT = 0.0;
         memo = nullptr;
+        stabMemo = nullptr;
+        flashMemo = nullptr;
     }
 
     NZ_HD const FlashOpts &O() const { return F->opt; }
@@ -1644,6 +1719,22 @@ struct Solver
 #pragma unroll
             for (int i = 0; i < NC; ++i)
                 res.incipient[p][i] = 0.0;
+        }
+        if (stabMemo)
+        {
+            bool hit = stabMemo->matches(P, T, zIn, active, activeX);
+#ifdef __CUDA_ARCH__
+            // warp-cooperative lanes take the stored answer together or not at all
+            if (width > 1)
+                hit = __all_sync(0xffffffffu, hit);
+#endif
+            if (hit)
+            {
+                res = stabMemo->res;
+                if (stabMemo->err)
+                    fail(stabMemo->err);
+                return;
+            }
         }
         if (!validatePT(P, T))
             return;
@@ -3188,6 +3279,22 @@ struct Solver
     template <bool TopLevel>
     NZ_HDN void flash(double P, double T, const double *zIn, Result<NC> &out)
     {
+        if (TopLevel && flashMemo)
+        {
+            bool hit = flashMemo->matches(P, T, zIn);
+#ifdef __CUDA_ARCH__
+            // warp-cooperative lanes take the stored answer together or not at all
+            if (width > 1)
+                hit = __all_sync(0xffffffffu, hit);
+#endif
+            if (hit)
+            {
+                out = flashMemo->r;
+                if (flashMemo->err)
+                    fail(flashMemo->err);
+                return;
+            }
+        }
         out.init();
         if (!validatePT(P, T))
             return;
@@ -3321,6 +3428,7 @@ struct Solver
                 if (perm[0] == roles[0] && perm[1] == roles[1] && perm[2] == roles[2])
                     continue;
                 Solver<NC> cand = *this;
+                cand.stabMemo = nullptr;   // stored tests were taken with the default roles
                 cand.roles[0] = perm[0];
                 cand.roles[1] = perm[1];
                 cand.roles[2] = perm[2];

@@ -1,6 +1,7 @@
 // nat_inst.cu -- Natural kernels of one component count (NZ_INST_NC).
 #include "natural_host.cuh"
 #include "natural_kernels.cuh"
+#include "natural_staged.cuh"
 
 #ifndef NZ_INST_NC
 #error "NZ_INST_NC must be defined"
@@ -40,10 +41,34 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
     case NAT_HISTORY:
         natHistoryKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.prevAcc, a.flag);
         break;
+    case NAT_UPDATE_PREPARE:
+        return natStagedStability<NC>(a.F, a.K, n, a.primary, a.ps, a.stagedScratch, smCount, st);
+    case NAT_UPDATE_REFLASH:
+    {
+        const NatStaged<NC> w = natStagedCarve<NC>(a.stagedScratch, n, a.F);
+        return natReflash<NC>(a.F, n, a.stagedScratch, a.flashScratch, a.reflashCount, w.a.evalCounter, smCount,
+                              st);
+    }
     case NAT_UPDATE:
+    {
+        StabilityMemo<NC> *memo = nullptr;
+        const FlashMemo<NC> *flashMemo = nullptr;
+        if (a.stagedScratch)
+        {
+            const NatStaged<NC> w = natStagedCarve<NC>(a.stagedScratch, n, a.F);
+            memo = w.memo;
+            flashMemo = w.flash;
+        }
         natUpdateKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.primary, a.ps, a.newPrimary, a.newPs,
-                                                           a.status, a.firstFailure, width);
+                                                           a.status, a.firstFailure, width, memo, flashMemo);
+        if (stagedDebugSync())
+        {
+            const cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess)
+                return cudaFail(e, "Natural update kernel");
+        }
         break;
+    }
     case NAT_INIT:
         natInitKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
                                                          a.firstFailure, width);
@@ -55,5 +80,26 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
     return e == cudaSuccess ? NZ_OK : cudaFail(e, "Natural kernel launch");
 }
 
+template <int NC>
+size_t natStagedBytesNc(int64_t n, const FluidDev &F)
+{
+    return natStagedBytes<NC>(n, F);
+}
+
+template <int NC>
+size_t natReflashBytesNc(int64_t n, const FluidDev &F)
+{
+    return natReflashBytes<NC>(n, F);
+}
+
+template <int NC>
+int *natReflashCountNc(void *scratch, int64_t n, const FluidDev &F)
+{
+    return natStagedCarve<NC>(scratch, n, F).count;
+}
+
 template int natLaunch<NZ_INST_NC>(int, const NatLaunch &, cudaStream_t);
+template size_t natStagedBytesNc<NZ_INST_NC>(int64_t, const FluidDev &);
+template size_t natReflashBytesNc<NZ_INST_NC>(int64_t, const FluidDev &);
+template int *natReflashCountNc<NZ_INST_NC>(void *, int64_t, const FluidDev &);
 } // namespace nz

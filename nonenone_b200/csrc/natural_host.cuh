@@ -14,6 +14,8 @@ enum NatOp
     NAT_HISTORY = 3,
     NAT_UPDATE = 4,
     NAT_INIT = 5,
+    NAT_UPDATE_PREPARE = 6,   // staged update: main-path stability tests, list of reflash cells
+    NAT_UPDATE_REFLASH = 7,   // staged update: batched flash of the listed cells
 };
 
 struct NatLaunch
@@ -33,8 +35,20 @@ struct NatLaunch
     int *flag;
     const double *initP;   // NAT_INIT: P[ncell], z[ncell][nc]
     const double *initZ;
+    void *stagedScratch;   // staged update: natStagedBytesNc<NC> bytes, or null for the per-cell update
+    void *flashScratch;    // NAT_UPDATE_REFLASH: natReflashBytesNc<NC>(reflashCount) bytes
+    int reflashCount;
 };
 
 template <int NC>
 int natLaunch(int op, const NatLaunch &a, cudaStream_t st);
+
+// Work space of the staged phase-state update of n cells, and of its batched
+// reflash of n cells; device address of the reflash count inside the former.
+template <int NC>
+size_t natStagedBytesNc(int64_t n, const FluidDev &F);
+template <int NC>
+size_t natReflashBytesNc(int64_t n, const FluidDev &F);
+template <int NC>
+int *natReflashCountNc(void *scratch, int64_t n, const FluidDev &F);
 } // namespace nz

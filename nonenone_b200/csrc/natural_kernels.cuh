@@ -223,10 +223,13 @@ NZ_BOTH uint8_t packOutcome(const UpdateOutcome &o)
 
 // sanitizePrimaryBeforeFlash + updatePhaseState of cell c into the scratch copy.
 // With width > 1, `width` lanes run the cell in lockstep and split the seeds of
-// its stability tests; lane 0 writes.
+// its stability tests; lane 0 writes.  With `memo` / `flashMemo`, a stability
+// test or top-level flash whose input matches memo[c] / flashMemo[c] takes its
+// stored answer.
 template <int NC>
 NZ_HD uint8_t cellUpdate(const FluidDev &F, const NatConst &K, const double *primary, const double *ps, int64_t c,
-                         double *newPrimary, double *newPs, int lane = 0, int width = 1)
+                         double *newPrimary, double *newPs, int lane = 0, int width = 1,
+                         StabilityMemo<NC> *memo = nullptr, const FlashMemo<NC> *flashMemo = nullptr)
 {
     using L = Layout<NC>;
     double a[L::B];
@@ -239,6 +242,8 @@ NZ_HD uint8_t cellUpdate(const FluidDev &F, const NatConst &K, const double *pri
     eq.s.setup(&F, F.salinity);
     eq.s.lane = lane;
     eq.s.width = width;
+    eq.s.stabMemo = memo ? memo + c : nullptr;
+    eq.s.flashMemo = flashMemo ? flashMemo + c : nullptr;
     eq.K = &K;
     eq.sanitize(a);
     UpdateOutcome o = eq.update(a, rec);
@@ -251,6 +256,27 @@ NZ_HD uint8_t cellUpdate(const FluidDev &F, const NatConst &K, const double *pri
         encodePhaseRec<NC>(rec, newPs + c * L::NPS);
     }
     return packOutcome(o);
+}
+
+// The head of cell c's update (decode, sanitize, updateHead) without any
+// flash or stability test: the input of the main-path stability test.  False
+// when the phase state cannot be decoded or a composition not normalised.
+template <int NC>
+NZ_HD bool cellUpdateHead(const FluidDev &F, const NatConst &K, const double *primary, const double *ps, int64_t c,
+                          UpdateHead<NC> &h)
+{
+    using L = Layout<NC>;
+    double a[L::B];
+    for (int r = 0; r < L::B; ++r)
+        a[r] = primary[c * L::B + r];
+    PhaseRec<NC> rec;
+    if (!decodePhaseRec<NC>(ps + c * L::NPS, rec))
+        return false;
+    Equilibrium<NC> eq;
+    eq.s.setup(&F, F.salinity);
+    eq.K = &K;
+    eq.sanitize(a);
+    return eq.updateHead(a, rec, h);
 }
 
 // initializeUniformFromPTZ per cell (natural_petsc_runtime_state.inc:107-164):
@@ -364,13 +390,14 @@ __global__ void __launch_bounds__(kNatBlock) natUpdateKernel(const __grid_consta
                                                              const __grid_constant__ NatConst K, int64_t ncell,
                                                              const double *primary, const double *ps,
                                                              double *newPrimary, double *newPs, uint8_t *status,
-                                                             unsigned long long *firstFailure, int width)
+                                                             unsigned long long *firstFailure, int width,
+                                                             StabilityMemo<NC> *memo, const FlashMemo<NC> *flashMemo)
 {
     const int lane = width == 32 ? int(threadIdx.x & 31) : 0;
     const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / width;
     if (c >= ncell)
         return;
-    const uint8_t s = cellUpdate<NC>(F, K, primary, ps, c, newPrimary, newPs, lane, width);
+    const uint8_t s = cellUpdate<NC>(F, K, primary, ps, c, newPrimary, newPs, lane, width, memo, flashMemo);
     if (lane != 0)
         return;
     status[c] = s;

@@ -77,6 +77,18 @@ NZ_HD void encodePhaseRec(const PhaseRec<NC> &r, double *ps)
     ps[L::psSuppression] = double(r.suppression);
 }
 
+// Result of the part of updatePhaseState before its first flash or test.
+template <int NC>
+struct UpdateHead
+{
+    double P;
+    double zt[NC];
+    double comps[3][NC];
+    uint8_t active;
+    uint8_t suppression;   // the phase state's suppression flags after the head
+    bool removed;
+};
+
 template <int NC>
 struct Equilibrium
 {
@@ -358,14 +370,14 @@ struct Equilibrium
         }
     }
 
-    // updatePhaseState (:282-503).  On failure the caller keeps its originals.
-    NZ_HDN UpdateOutcome update(double *primary, PhaseRec<NC> &ps)
+    // The part of updatePhaseState (:282-335) before any flash or stability
+    // test: SW role orientation, the overall composition, removal of phases
+    // whose Newton saturation fell to 1e-4 and the present phases'
+    // compositions.  False when a composition cannot be normalised.
+    NZ_HDN bool updateHead(double *primary, PhaseRec<NC> &ps, UpdateHead<NC> &h)
     {
-        UpdateOutcome out{UPD_UPDATED, false, false, false, false, false};
-        const double T = K->temperature;
         canonicalizeSwRoles(primary, ps);
-        double zt[NC];
-        transitionOverall(primary, ps, zt);
+        transitionOverall(primary, ps, h.zt);
         uint8_t active = ps.presence;
         ps.suppression &= uint8_t(~active);
         bool removed = false;
@@ -389,17 +401,34 @@ struct Equilibrium
             primary[satIndex(survivor)] = 1.0;
             removed = true;
         }
-        out.phaseRemoved = removed;
+        h.active = active;
+        h.removed = removed;
         ps.presence = active;
         for (int i = 0; i < NC; ++i)
-            ps.z[i] = zt[i];
-        double comps[3][NC];
-        phaseCompositions(primary, comps);
-        if (s.err)
+            ps.z[i] = h.zt[i];
+        phaseCompositions(primary, h.comps);
+        h.P = primary[0];
+        h.suppression = ps.suppression;
+        return !s.err;
+    }
+
+    // updatePhaseState (:282-503).  On failure the caller keeps its originals.
+    NZ_HDN UpdateOutcome update(double *primary, PhaseRec<NC> &ps)
+    {
+        UpdateOutcome out{UPD_UPDATED, false, false, false, false, false};
+        const double T = K->temperature;
+        UpdateHead<NC> h;
+        const bool headOk = updateHead(primary, ps, h);
+        out.phaseRemoved = h.removed;
+        if (!headOk)
         {
             out.status = UPD_FAILED;
             return out;
         }
+        const double *zt = h.zt;
+        uint8_t active = h.active;
+        const bool removed = h.removed;
+        double (&comps)[3][NC] = h.comps;
         const double P = primary[0];
         if (removed)
         {

@@ -20,6 +20,7 @@
 // Selected names only: a namespace-wide using would put nz's double math
 // overloads beside the CUDA headers' own.
 using nz::cudaFail;
+using nz::FluidDev;
 using nz::kCentipoise;
 using nz::kKelvinPerRankine;
 using nz::kPsi;
@@ -29,7 +30,12 @@ using nz::NAT_INIT;
 using nz::NAT_JACOBIAN;
 using nz::NAT_RESIDUAL;
 using nz::NAT_UPDATE;
+using nz::NAT_UPDATE_PREPARE;
+using nz::NAT_UPDATE_REFLASH;
 using nz::natLaunch;
+using nz::natStagedBytesNc;
+using nz::natReflashBytesNc;
+using nz::natReflashCountNc;
 using nz::NatConst;
 using nz::NatGeom;
 using nz::NatLaunch;
@@ -49,12 +55,17 @@ struct nz_natural
     double *prevAcc{nullptr}, *cache{nullptr}, *newPrimary{nullptr}, *newPs{nullptr};
     uint8_t *status{nullptr};
     unsigned long long *firstFailure{nullptr};
+    unsigned char *staged{nullptr};   // work space of the staged update (tests, memos, reflash list)
+    bool stagedUpdate{true};
+    void *reflash{nullptr};           // work space of the update's batched reflash, grown on demand
+    size_t reflashBytes{0};
     int *flag{nullptr};
     nz_report *report{nullptr};
     // pinned host mirror of flag / report
     struct Pinned
     {
         int flag;
+        int reflashCount;
         nz_report report;
     } *pinned{nullptr};
     std::vector<void *> allocations;
@@ -113,6 +124,8 @@ struct nz_natural
     {
         for (void *p : allocations)
             cudaFree(p);
+        if (reflash)
+            cudaFree(reflash);
         if (pinned)
             cudaFreeHost(pinned);
     }
@@ -120,6 +133,45 @@ struct nz_natural
 
 namespace
 {
+size_t natStagedBytesFor(int nc, int64_t n, const FluidDev &F)
+{
+    switch (nc)
+    {
+    case 3: return natStagedBytesNc<3>(n, F);
+    case 4: return natStagedBytesNc<4>(n, F);
+    case 5: return natStagedBytesNc<5>(n, F);
+    case 6: return natStagedBytesNc<6>(n, F);
+    case 8: return natStagedBytesNc<8>(n, F);
+    default: return 0;
+    }
+}
+
+size_t natReflashBytesFor(int nc, int64_t n, const FluidDev &F)
+{
+    switch (nc)
+    {
+    case 3: return natReflashBytesNc<3>(n, F);
+    case 4: return natReflashBytesNc<4>(n, F);
+    case 5: return natReflashBytesNc<5>(n, F);
+    case 6: return natReflashBytesNc<6>(n, F);
+    case 8: return natReflashBytesNc<8>(n, F);
+    default: return 0;
+    }
+}
+
+int *natReflashCountFor(int nc, void *scratch, int64_t n, const FluidDev &F)
+{
+    switch (nc)
+    {
+    case 3: return natReflashCountNc<3>(scratch, n, F);
+    case 4: return natReflashCountNc<4>(scratch, n, F);
+    case 5: return natReflashCountNc<5>(scratch, n, F);
+    case 6: return natReflashCountNc<6>(scratch, n, F);
+    case 8: return natReflashCountNc<8>(scratch, n, F);
+    default: return nullptr;
+    }
+}
+
 int natDispatch(int nc, int op, const NatLaunch &a, cudaStream_t st)
 {
     switch (nc)
@@ -131,6 +183,43 @@ int natDispatch(int nc, int op, const NatLaunch &a, cudaStream_t st)
     case 8: return natLaunch<8>(op, a, st);
     default: return setError(NZ_ERR_UNSUPPORTED, "nc=%d not compiled", nc);
     }
+}
+
+// The staged update's preparation: main-path stability tests on the trial
+// kernels, then the batched flash of the cells that reflash.  Synchronises
+// once, to size the reflash batch.
+int natPrepareStagedUpdate(nz_natural *nat, NatLaunch &a, cudaStream_t st)
+{
+    a.stagedScratch = nat->staged;
+    int rc = natDispatch(nat->nc, NAT_UPDATE_PREPARE, a, st);
+    if (rc != NZ_OK)
+        return rc;
+    const FluidDev &F = nat->ctx->fluid;
+    cudaError_t e = cudaMemcpyAsync(&nat->pinned->reflashCount, natReflashCountFor(nat->nc, nat->staged, nat->ncell, F),
+                                    sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return cudaFail(e, "nz_update_state: reflash count");
+    const int n = int(std::min<int64_t>(std::max(nat->pinned->reflashCount, 0), nat->ncell));
+    if (n == 0)
+        return NZ_OK;
+    const size_t need = natReflashBytesFor(nat->nc, n, F);
+    if (need > nat->reflashBytes)
+    {
+        if (nat->reflash)
+            cudaFree(nat->reflash);
+        nat->reflash = nullptr;
+        nat->reflashBytes = 0;
+        const size_t grow = need + need / 4;   // room for the next iterate's count
+        e = cudaMalloc(&nat->reflash, grow);
+        if (e != cudaSuccess)
+            return cudaFail(e, "nz_update_state: reflash work space");
+        nat->reflashBytes = grow;
+    }
+    a.flashScratch = nat->reflash;
+    a.reflashCount = n;
+    return natDispatch(nat->nc, NAT_UPDATE_REFLASH, a, st);
 }
 
 // Count the StableReducedSet cells before the first failure and fill the report.
@@ -333,7 +422,8 @@ int nz_natural_create(nz_ctx *ctx, const nz_natural_desc *desc, nz_natural **out
         (rc = nat->alloc(nat->cache, n * cacheFields)) || (rc = nat->alloc(nat->newPrimary, n * nat->B)) ||
         (rc = nat->alloc(nat->newPs, n * nat->NPS)) || (rc = nat->alloc(nat->status, n)) ||
         (rc = nat->alloc(nat->firstFailure, 1)) || (rc = nat->alloc(nat->flag, 1)) ||
-        (rc = nat->alloc(nat->report, 1)))
+        (rc = nat->alloc(nat->report, 1)) ||
+        (rc = nat->alloc(nat->staged, natStagedBytesFor(nc, n, ctx->fluid))))
     {
         delete nat;
         return rc;
@@ -354,6 +444,14 @@ int nz_natural_destroy(nz_natural *nat)
         return NZ_OK;
     cudaSetDevice(nat->ctx->device);
     delete nat;
+    return NZ_OK;
+}
+
+int nz_natural_set_staged_update(nz_natural *nat, int32_t enabled)
+{
+    if (!nat)
+        return setError(NZ_ERR_ARGUMENT, "nz_natural_set_staged_update: null argument");
+    nat->stagedUpdate = enabled != 0;
     return NZ_OK;
 }
 
@@ -444,7 +542,10 @@ int nz_update_state(nz_natural *nat, double *primary, double *phase_state, nz_re
     a.newPs = nat->newPs;
     a.status = nat->status;
     a.firstFailure = nat->firstFailure;
-    int rc = natDispatch(nat->nc, NAT_UPDATE, a, st);
+    int rc = NZ_OK;
+    if (nat->stagedUpdate && (rc = natPrepareStagedUpdate(nat, a, st)) != NZ_OK)
+        return rc;
+    rc = natDispatch(nat->nc, NAT_UPDATE, a, st);
     if (rc != NZ_OK)
         return rc;
     natReportKernel<<<1, 256, 0, st>>>(nat->ncell, nat->status, nat->firstFailure, nat->report);

@@ -99,6 +99,12 @@ class NaturalAssembler:
         return check(self.lib.nz_natural_set_history(self.handle, _ptr(p), _ptr(s), _stream_ptr(stream)),
                      "nz_natural_set_history")
 
+    def set_staged_update(self, enabled: bool):
+        """Run each cell's first stability test of the update on the batched
+        trial kernels (default) or inside the per-cell update code."""
+        check(self.lib.nz_natural_set_staged_update(self.handle, 1 if enabled else 0),
+              "nz_natural_set_staged_update")
+
     def update_state_with_report(self, primary, phase_state, stream=None):
         """Transactional phase-state update in place.  Returns (rc, report):
         rc 0 = committed, 1 = recoverable failure (nothing committed)."""

@@ -3,9 +3,11 @@
   python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged]
       one N-point batch of the seeded flash mixture (after a 4,096-point warm-up
       batch, so kernels of the measured batch come second)
-  python -m nonenone_b200.profile_cases natural NX NY NZ
+  python -m nonenone_b200.profile_cases natural NX NY NZ [--update] [--per-cell]
       P-T-z initialisation of an NX x NY x NZ grid of the H2O/CO2/nC10 case,
-      then two residual + Jacobian evaluations of the accepted state
+      then two residual + Jacobian evaluations of the accepted state; with
+      --update first one transactional phase-state update of a perturbed
+      iterate (staged, or with every test inside the per-cell code)
 """
 from __future__ import annotations
 
@@ -36,7 +38,7 @@ def run_flash(n: int, precision: str) -> None:
           f"{fl.eos_eval_count()} EOS evaluations")
 
 
-def run_natural(nx: int, ny: int, nz: int) -> None:
+def run_natural(nx: int, ny: int, nz: int, update: bool = False, per_cell: bool = False) -> None:
     import torch
     from . import abi, synth
     from .flash import Context, CubicThreePhaseFlash
@@ -53,6 +55,17 @@ def run_natural(nx: int, ny: int, nz: int) -> None:
     P[bad], z[bad] = P[good[:bad.size]], z[good[:bad.size]]
     primary, ps = nat.initialize_from_ptz(P, z)
     nat.refresh_history(primary, ps)
+    if update:
+        nat.set_staged_update(not per_cell)
+        cur = torch.as_tensor(synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), fluid.nc, 11, 1.0),
+                              device=primary.device)
+        work_s = ps.clone()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        rc, rep = nat.update_state_with_report(cur, work_s)
+        b.record()
+        torch.cuda.synchronize()
+        print(f"update of {grid.ncell} cells: {a.elapsed_time(b):.1f} ms, committed {rc == 0}")
     vals = torch.empty(nat.nnzb, nat.B, nat.B, dtype=torch.float64, device=primary.device)
     F = torch.empty_like(primary)
     for _ in range(2):
@@ -73,11 +86,13 @@ def main(argv=None) -> int:
     nat.add_argument("nx", type=int)
     nat.add_argument("ny", type=int)
     nat.add_argument("nz", type=int)
+    nat.add_argument("--update", action="store_true")
+    nat.add_argument("--per-cell", action="store_true")
     a = ap.parse_args(argv)
     if a.case == "flash":
         run_flash(a.n, a.precision)
     else:
-        run_natural(a.nx, a.ny, a.nz)
+        run_natural(a.nx, a.ny, a.nz, a.update, a.per_cell)
     return 0
 
 

@@ -139,6 +139,30 @@ def test_update_state(case, torch_cuda):
     assert_state(cur.cpu().numpy(), ps.cpu().numpy(), g["updated_primary"], g["updated_phase_state"], name)
 
 
+def test_update_state_per_cell_tests(case, torch_cuda):
+    """The update with every stability test inside the per-cell code (the
+    staged trial kernels switched off) gives the same report and states."""
+    torch = torch_cuda
+    name, g, nat = case
+    nat.set_staged_update(False)
+    try:
+        for it in ("current", "failing"):
+            cur = torch.as_tensor(g[it], device="cuda").clone()
+            ps = torch.as_tensor(g["phase_state"], device="cuda").clone()
+            rc, rep = nat.update_state_with_report(cur, ps)
+            want = g["report"] if it == "current" else g["failing_report"]
+            got = np.array([getattr(rep, f) for f in REPORT_FIELDS])
+            assert np.array_equal(got, want), (it, dict(zip(REPORT_FIELDS, zip(got, want))))
+            if it == "current":
+                assert rc == 0
+                assert_state(cur.cpu().numpy(), ps.cpu().numpy(), g["updated_primary"],
+                             g["updated_phase_state"], name + " per-cell tests")
+            else:
+                assert rc == 1
+    finally:
+        nat.set_staged_update(True)
+
+
 def test_update_state_failure_commits_nothing(case, torch_cuda):
     torch = torch_cuda
     name, g, nat = case
