@@ -200,9 +200,9 @@ def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: boo
         t_jac = sorted(timed(lambda: nat.assemble_jacobian(cur, ps, values=vals)) for _ in range(max(n_rep, 3)))
         t_newton = sorted(timed(newton) for _ in range(n_rep))
         # the same update with every stability test inside the per-cell code
-        nat.set_staged_update(False)
+        nat.set_update_mode("per_cell")
         t_update_per_cell = timed(update)
-        nat.set_staged_update(True)
+        nat.set_update_mode("auto")
         rc, rep = update()
         jac_bytes = nat.nnzb * nat.B * nat.B * 8 + grid.ncell * nat.B * 8
         jac_ms = t_jac[len(t_jac) // 2]
@@ -211,7 +211,8 @@ def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: boo
             "newton_eval_ms": {"p50": t_newton[len(t_newton) // 2], "max": t_newton[-1], "reps": n_rep},
             "cell_evals_per_s": grid.ncell / (t_newton[len(t_newton) // 2] * 1e-3),
             "update_ms": t_update[len(t_update) // 2],
-            "update_ms_per_cell_tests": t_update_per_cell,
+            "update_form": "staged" if grid.ncell >= 148 * 256 else "per-cell (warp per cell)",
+            "update_ms_per_cell_form": t_update_per_cell,
             "residual_ms": t_res[len(t_res) // 2],
             "jacobian_ms": jac_ms,
             "update_committed": rc == 0,

@@ -306,14 +306,23 @@ int nz_natural_init_ptz(nz_natural* nat, const double* P, const double* z,
 int nz_natural_set_history(nz_natural* nat, const double* primary,
                            const double* phase_state, void* stream);
 /* Transactional phase-state update of every cell; commits all cells or none.
- * By default the first stability test of every cell runs on the batched
- * lane-per-trial kernels (work space held by the nz_natural from its
- * creation: 2.5 KB per cell for nc = 3, 4.6 KB for nc = 6, 6.2 KB for
- * nc = 8); results are those of the per-cell tests, which
- * nz_natural_set_staged_update(nat, 0) selects instead. */
+ * Two equivalent forms (same results):
+ *   staged    every cell's stability test runs on the batched lane-per-trial
+ *             kernels and every reflash on the staged batched flash, then the
+ *             per-cell code takes those answers (work space held by the
+ *             nz_natural from its creation: about 2.8 KB per cell for nc = 3,
+ *             5.0 KB for nc = 6, 6.8 KB for nc = 8, plus the reflash batch's,
+ *             grown on demand; one host synchronisation to size that batch);
+ *   per-cell  each cell runs its whole update in one thread (a warp per cell
+ *             on grids below 256 cells per SM).
+ * NZ_UPDATE_AUTO (the default) takes the staged form from 256 cells per SM,
+ * where the per-cell form runs one thread per cell. */
 int nz_update_state(nz_natural* nat, double* primary, double* phase_state,
                     nz_report* report, void* stream);
-int nz_natural_set_staged_update(nz_natural* nat, int32_t enabled);
+#define NZ_UPDATE_PER_CELL 0
+#define NZ_UPDATE_STAGED 1
+#define NZ_UPDATE_AUTO 2
+int nz_natural_set_update_mode(nz_natural* nat, int32_t mode);
 /* Residual F[ncell*B] (cell-major). */
 int nz_residual(nz_natural* nat, const double* primary,
                 const double* phase_state, double* residual, void* stream);

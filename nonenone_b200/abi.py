@@ -157,3 +157,8 @@ def block_size(nc: int) -> int:
 def phase_state_size(nc: int) -> int:
     """PetscPhaseStateCodec doubles per cell (indices.hpp:227-278)."""
     return 3 * nc + 8
+
+# nz_natural_set_update_mode modes
+UPDATE_PER_CELL = 0
+UPDATE_STAGED = 1
+UPDATE_AUTO = 2

@@ -1,29 +1,36 @@
-// natural_staged.cuh -- the Natural phase-state update with its main-path
-// stability tests on the lane-per-trial kernel of the staged flash.
+// natural_staged.cuh -- the Natural phase-state update with its stability
+// tests on the lane-per-trial kernel and its reflashes on the staged batched
+// flash.
 //
 // updateStateWithReport (natural_petsc_runtime_state.inc:166-345) runs
-// updatePhaseState on every cell, and every cell that keeps fewer than three
-// phases runs a multi-seed TPD stability test (three_phase_equilibrium.hpp:
-// 282-503).  One thread per cell runs those trials at a few active lanes per
-// warp.  Here the update takes three steps:
+// updatePhaseState on every cell.  A cell that keeps fewer than three phases
+// runs a multi-seed TPD stability test (three_phase_equilibrium.hpp:467-487);
+// a cell whose Newton saturation removed a phase first runs a restricted flash
+// and tests its result (:398-463); an unstable or invalid test ends in a full
+// P-T-z flash of the cell.  One thread per cell runs all of this at a few
+// active lanes per warp.  Here the update takes four steps:
 //
 //   prefix    the head of every cell's update (decode, sanitize and the part
 //             of updatePhaseState before any flash: Equilibrium::updateHead)
-//             yields the input of the cell's main-path test when no phase was
-//             removed; it is recorded in a StabilityMemo, the test's
-//             reference-phase data prepared (Driver::prepareStability) and one
-//             task per missing phase queued;
+//             yields the input of the main-path test; cells that removed a
+//             phase are listed and a second kernel runs their restricted flash
+//             (the same Solver::flashRestricted on the same input) for the
+//             input of theirs.  Each input is recorded in a StabilityMemo, the
+//             test's reference-phase data prepared (Driver::prepareStability)
+//             and one task per missing phase queued;
 //   trials    stagedTrialKernel runs every (cell, missing phase, seed) trial
 //             as its own lane; a combine kernel folds them in seed order
 //             (Driver::combineStability) into the memo;
-//   update    the per-cell code runs from the start; its stability test finds
-//             the memo with the identical input and takes the answer; every
-//             other test of the cell (phase-removal path, reflash) runs inline.
+//   reflash   the cells whose answer calls for a full flash are listed and
+//             flashed by the staged batched flash into per-cell FlashMemos;
+//   update    the per-cell code runs from the start; its stability test and
+//             its top-level flash find the memos with the identical input and
+//             take the answers; anything else runs inline.
 //
-// The update computes the test's input with the same updateHead, so the input
-// matches bit for bit, and the combined answer equals the sequential test's
-// (the staged flash relies on the same equivalence).  A test whose input does
-// not match simply runs inline.
+// The update computes every recorded input with the same functions on the same
+// data, so the inputs match bit for bit; the combined test equals the
+// sequential test and the staged flash equals flash() (the staged flash relies
+// on the same equivalences).  An input that does not match simply runs inline.
 #pragma once
 
 #include "natural_kernels.cuh"
@@ -49,8 +56,18 @@ size_t natStagedBytes(int64_t n, const FluidDev &F)
     add(size_t(n));                      // suppression flags after the update head
     add(sizeof(int64_t) * size_t(n));    // cells whose update reflashes
     add(sizeof(int));                    // their count
+    add(sizeof(int64_t) * size_t(n));    // cells whose head removed a phase
+    add(sizeof(int));                    // their count
+    add(size_t(n));                      // path of each cell's recorded test
     return b;
 }
+
+// Which stability test a cell's memo holds, and what follows it in the update
+// (three_phase_equilibrium.hpp:400-487).
+constexpr uint8_t PATH_NONE = 0;      // nothing recorded: the update runs inline
+constexpr uint8_t PATH_MAIN = 1;      // the main-path test of the active set
+constexpr uint8_t PATH_REMOVED = 2;   // the test of the restricted flash's set after a phase removal
+constexpr uint8_t PATH_REFLASH = 3;   // phase removed, restricted flash not converged: reflash directly
 
 // The carved work space of the staged update.
 template <int NC>
@@ -62,6 +79,9 @@ struct NatStaged
     uint8_t *supp;
     int64_t *cells;
     int *count;
+    int64_t *removed;
+    int *removedCount;
+    uint8_t *path;
 };
 
 template <int NC>
@@ -88,7 +108,56 @@ NatStaged<NC> natStagedCarve(void *scratch, int64_t n, const FluidDev &F)
     w.supp = reinterpret_cast<uint8_t *>(take(size_t(n)));
     w.cells = reinterpret_cast<int64_t *>(take(sizeof(int64_t) * size_t(n)));
     w.count = reinterpret_cast<int *>(take(sizeof(int)));
+    w.removed = reinterpret_cast<int64_t *>(take(sizeof(int64_t) * size_t(n)));
+    w.removedCount = reinterpret_cast<int *>(take(sizeof(int)));
+    w.path = reinterpret_cast<uint8_t *>(take(size_t(n)));
     return w;
+}
+
+// Record a cell's stability test (input, suppression flags, path), prepare its
+// reference-phase data and queue one trial task per missing phase; a test
+// that resolves without trials is stored as answered.
+template <int NC>
+__device__ void natRecordTest(const FluidDev &F, double T, int64_t ncell, const NatStaged<NC> &w, int64_t c, double P,
+                              const double *z, uint8_t active, const double (&x)[3][NC], uint8_t suppression,
+                              uint8_t path)
+{
+    const StagedArgs &a = w.a;
+    StabilityMemo<NC> &m = w.memo[c];
+    m.record(P, T, z, active, x);
+    w.supp[c] = suppression;
+    w.path[c] = path;
+    DriverState<NC> &st = static_cast<DriverState<NC> *>(a.states)[c];
+    st.P = P;
+    st.T = T;
+    st.sal = F.salinity;
+    Driver<NC> d;
+    d.s.setup(&F, F.salinity);
+    d.st = &st;
+    for (int i = 0; i < NC; ++i)
+        st.z[i] = z[i];
+    d.s.normalize(st.z);   // the seeds use the normalised feed, as stabilityTest does
+    StabilityResult<NC> res;
+    if (!d.prepareStability(P, T, z, active, x, res) || d.s.err != ERR_NONE)
+    {
+        m.res = res;
+        m.err = d.s.err;
+        m.state = MEMO_READY;
+        return;
+    }
+    int missing = 0;
+    for (int cand = 0; cand < 3; ++cand)
+        if (!(active & bitOf(cand)))
+            ++missing;
+    int slot = atomicAdd(&a.counters[0], missing);
+    if (slot < 0 || int64_t(slot) + missing > 3 * ncell)
+    {
+        atomicExch(&a.counters[kCounterBound], 21);   // self-check: the queue holds 3 tasks per cell
+        return;
+    }
+    for (int cand = 0; cand < 3; ++cand)
+        if (!(active & bitOf(cand)))
+            a.tasks[0][slot++] = (static_cast<unsigned long long>(c) << 2) | unsigned(cand);
 }
 
 // Prefix pass: record each cell's main-path stability test and queue its trials.
@@ -106,42 +175,59 @@ __global__ void __launch_bounds__(kNatBlock) natPrefixKernel(const __grid_consta
     m.state = MEMO_NONE;
     m.err = ERR_NONE;
     w.flash[c].valid = 0;
+    w.path[c] = PATH_NONE;
     UpdateHead<NC> h;
-    if (!cellUpdateHead<NC>(F, K, primary, ps, c, h) || h.removed || popcount3(h.active) == 3)
+    if (!cellUpdateHead<NC>(F, K, primary, ps, c, h))
         return;
-    m.record(h.P, K.temperature, h.zt, h.active, h.comps);
-    w.supp[c] = h.suppression;
-    DriverState<NC> &st = static_cast<DriverState<NC> *>(a.states)[c];
-    st.P = h.P;
-    st.T = K.temperature;
-    st.sal = F.salinity;
-    Driver<NC> d;
-    d.s.setup(&F, F.salinity);
-    d.st = &st;
-    for (int i = 0; i < NC; ++i)
-        st.z[i] = h.zt[i];
-    d.s.normalize(st.z);   // the seeds use the normalised feed, as stabilityTest does
-    StabilityResult<NC> res;
-    if (!d.prepareStability(h.P, K.temperature, h.zt, h.active, h.comps, res) || d.s.err != ERR_NONE)
+    if (h.removed)
     {
-        m.res = res;
-        m.err = d.s.err;
-        m.state = MEMO_READY;
+        const int k = atomicAdd(w.removedCount, 1);
+        if (k >= 0 && k < ncell)
+            w.removed[k] = c;
         return;
     }
-    int missing = 0;
-    for (int cand = 0; cand < 3; ++cand)
-        if (!(h.active & bitOf(cand)))
-            ++missing;
-    int slot = atomicAdd(&a.counters[0], missing);
-    if (slot < 0 || int64_t(slot) + missing > 3 * ncell)
+    if (popcount3(h.active) == 3)
+        return;
+    natRecordTest<NC>(F, K.temperature, ncell, w, c, h.P, h.zt, h.active, h.comps, h.suppression, PATH_MAIN);
+}
+
+// Cells whose head removed a phase: their restricted flash (the same
+// Solver::flashRestricted the update runs, on the same input) gives the set
+// and compositions of the test that follows it.
+template <int NC>
+__global__ void __launch_bounds__(kNatBlock) natRemovedKernel(const __grid_constant__ FluidDev F,
+                                                              const __grid_constant__ NatConst K, int64_t ncell,
+                                                              const double *primary, const double *ps,
+                                                              const __grid_constant__ NatStaged<NC> w)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int listed = *w.removedCount;
+    if (k >= listed || k >= ncell)
+        return;
+    const int64_t c = w.removed[k];
+    if (c < 0 || c >= ncell)
+        return;
+    UpdateHead<NC> h;
+    if (!cellUpdateHead<NC>(F, K, primary, ps, c, h))
+        return;
+    Solver<NC> s;
+    s.setup(&F, F.salinity);
+    Result<NC> reduced;
+    s.flashRestricted(h.P, K.temperature, h.zt, h.active, &h.comps, reduced);
+    if (s.err)
+        return;   // the update fails this cell inline
+    if (!reduced.converged)
     {
-        atomicExch(&a.counters[kCounterBound], 21);   // self-check: the queue holds 3 tasks per cell
+        StabilityMemo<NC> &m = w.memo[c];
+        m.record(h.P, K.temperature, h.zt, 0, reduced.x);
+        m.state = MEMO_NONE;   // no test: the flash input only
+        w.path[c] = PATH_REFLASH;
         return;
     }
-    for (int cand = 0; cand < 3; ++cand)
-        if (!(h.active & bitOf(cand)))
-            a.tasks[0][slot++] = (static_cast<unsigned long long>(c) << 2) | unsigned(cand);
+    if (popcount3(reduced.presence) == 3)
+        return;
+    natRecordTest<NC>(F, K.temperature, ncell, w, c, h.P, h.zt, reduced.presence, reduced.x, h.suppression,
+                      PATH_REMOVED);
 }
 
 // Fold each cell's trials into its memo.  A trial kernel that tripped its
@@ -178,11 +264,19 @@ __global__ void __launch_bounds__(kNatBlock) natSelectKernel(int64_t ncell, cons
     if (c >= ncell)
         return;
     const StabilityMemo<NC> &m = w.memo[c];
-    if (m.state != MEMO_READY || m.err != ERR_NONE)
+    const uint8_t path = w.path[c];
+    if (path == PATH_NONE)
         return;
-    const bool invalid = !m.res.valid;
-    if (!invalid && !Equilibrium<NC>::strongInstability(m.res, m.active, w.supp[c]))
-        return;
+    if (path != PATH_REFLASH)
+    {
+        if (m.state != MEMO_READY || m.err != ERR_NONE)
+            return;
+        // main path: invalid or unstable; removed path: the same condition
+        // (unstableMissing, :400-420)
+        const bool invalid = !m.res.valid;
+        if (!invalid && !Equilibrium<NC>::strongInstability(m.res, m.active, w.supp[c]))
+            return;
+    }
     const int k = atomicAdd(w.count, 1);
     if (k >= 0 && k < ncell)
         w.cells[k] = c;
@@ -305,6 +399,8 @@ int natStagedStability(const FluidDev &F, const NatConst &K, int64_t ncell, cons
         e = cudaMemsetAsync(a.evalCounter, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(w.count, 0, sizeof(int), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(w.removedCount, 0, sizeof(int), st);
     if (e != cudaSuccess)
         return cudaFail(e, "Natural staged update");
     // NZ_STAGED_SYNC=1: synchronise after every launch and name the one that failed
@@ -328,6 +424,9 @@ int natStagedStability(const FluidDev &F, const NatConst &K, int64_t ncell, cons
     natPrefixKernel<NC><<<grid, kNatBlock, 0, st>>>(F, K, ncell, primary, ps, w);
     int rc = after("Natural staged update: prefix");
     if (rc != NZ_OK)
+        return rc;
+    natRemovedKernel<NC><<<grid, kNatBlock, 0, st>>>(F, K, ncell, primary, ps, w);
+    if ((rc = after("Natural staged update: removed-phase cells")) != NZ_OK)
         return rc;
     stagedTrialKernel<NC><<<unsigned(smCount * kTrialBlocksPerSm), kTrialBlock, 0, st>>>(F, a, 0);
     if ((rc = after("Natural staged update: trials")) != NZ_OK)

@@ -56,7 +56,7 @@ struct nz_natural
     uint8_t *status{nullptr};
     unsigned long long *firstFailure{nullptr};
     unsigned char *staged{nullptr};   // work space of the staged update (tests, memos, reflash list)
-    bool stagedUpdate{true};
+    int updateMode{NZ_UPDATE_AUTO};
     void *reflash{nullptr};           // work space of the update's batched reflash, grown on demand
     size_t reflashBytes{0};
     int *flag{nullptr};
@@ -447,11 +447,13 @@ int nz_natural_destroy(nz_natural *nat)
     return NZ_OK;
 }
 
-int nz_natural_set_staged_update(nz_natural *nat, int32_t enabled)
+int nz_natural_set_update_mode(nz_natural *nat, int32_t mode)
 {
     if (!nat)
-        return setError(NZ_ERR_ARGUMENT, "nz_natural_set_staged_update: null argument");
-    nat->stagedUpdate = enabled != 0;
+        return setError(NZ_ERR_ARGUMENT, "nz_natural_set_update_mode: null argument");
+    if (mode != NZ_UPDATE_PER_CELL && mode != NZ_UPDATE_STAGED && mode != NZ_UPDATE_AUTO)
+        return setError(NZ_ERR_ARGUMENT, "nz_natural_set_update_mode: unknown mode %d", int(mode));
+    nat->updateMode = mode;
     return NZ_OK;
 }
 
@@ -543,7 +545,14 @@ int nz_update_state(nz_natural *nat, double *primary, double *phase_state, nz_re
     a.status = nat->status;
     a.firstFailure = nat->firstFailure;
     int rc = NZ_OK;
-    if (nat->stagedUpdate && (rc = natPrepareStagedUpdate(nat, a, st)) != NZ_OK)
+    bool staged = nat->updateMode == NZ_UPDATE_STAGED;
+    if (nat->updateMode == NZ_UPDATE_AUTO)
+    {
+        int smCount = 148;
+        cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, nat->ctx->device);
+        staged = nat->ncell >= int64_t(smCount) * 256;
+    }
+    if (staged && (rc = natPrepareStagedUpdate(nat, a, st)) != NZ_OK)
         return rc;
     rc = natDispatch(nat->nc, NAT_UPDATE, a, st);
     if (rc != NZ_OK)

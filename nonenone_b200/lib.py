@@ -19,7 +19,7 @@ EXPORTED = (
     "nz_flash_eos_eval_count", "nz_stability_batch", "nz_natural_create",
     "nz_natural_destroy", "nz_natural_pattern", "nz_natural_set_history",
     "nz_update_state", "nz_residual", "nz_jacobian", "nz_diag_fma_peak",
-    "nz_flash_batch_noalloc", "nz_natural_init_ptz", "nz_natural_set_staged_update",
+    "nz_flash_batch_noalloc", "nz_natural_init_ptz", "nz_natural_set_update_mode",
 )
 
 _lib = None
@@ -56,7 +56,7 @@ def load():
         L.nz_natural_init_ptz.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.nz_natural_set_history.argtypes = [vp, vp, vp, vp]
         L.nz_update_state.argtypes = [vp, vp, vp, vp, vp]
-        L.nz_natural_set_staged_update.argtypes = [vp, i32]
+        L.nz_natural_set_update_mode.argtypes = [vp, i32]
         L.nz_residual.argtypes = [vp, vp, vp, vp, vp]
         L.nz_jacobian.argtypes = [vp, vp, vp, vp, vp, vp]
     L.nz_diag_fma_peak.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]

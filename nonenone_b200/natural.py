@@ -99,11 +99,13 @@ class NaturalAssembler:
         return check(self.lib.nz_natural_set_history(self.handle, _ptr(p), _ptr(s), _stream_ptr(stream)),
                      "nz_natural_set_history")
 
-    def set_staged_update(self, enabled: bool):
-        """Run each cell's first stability test of the update on the batched
-        trial kernels (default) or inside the per-cell update code."""
-        check(self.lib.nz_natural_set_staged_update(self.handle, 1 if enabled else 0),
-              "nz_natural_set_staged_update")
+    def set_update_mode(self, mode: str):
+        """Form of update_state_with_report: "staged" (stability tests on the
+        batched trial kernels, reflashes on the staged flash), "per_cell"
+        (the whole update per cell) or "auto" (staged from 256 cells per SM,
+        the default).  Both forms give the same results."""
+        code = {"per_cell": abi.UPDATE_PER_CELL, "staged": abi.UPDATE_STAGED, "auto": abi.UPDATE_AUTO}[mode]
+        check(self.lib.nz_natural_set_update_mode(self.handle, code), "nz_natural_set_update_mode")
 
     def update_state_with_report(self, primary, phase_state, stream=None):
         """Transactional phase-state update in place.  Returns (rc, report):

@@ -56,7 +56,7 @@ def run_natural(nx: int, ny: int, nz: int, update: bool = False, per_cell: bool 
     primary, ps = nat.initialize_from_ptz(P, z)
     nat.refresh_history(primary, ps)
     if update:
-        nat.set_staged_update(not per_cell)
+        nat.set_update_mode("per_cell" if per_cell else "staged")
         cur = torch.as_tensor(synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), fluid.nc, 11, 1.0),
                               device=primary.device)
         work_s = ps.clone()

@@ -53,6 +53,7 @@ def assembler(fluid, grid, time_step=864.0, temperature=353.15):
     nat = NaturalAssembler(ctx, grid, time_step, temperature,
                            abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10))
     nat._ctx_keep = ctx
+    nat.set_update_mode("staged")   # the parity tests run the staged form on every grid size
     return nat
 
 
@@ -140,11 +141,11 @@ def test_update_state(case, torch_cuda):
 
 
 def test_update_state_per_cell_tests(case, torch_cuda):
-    """The update with every stability test inside the per-cell code (the
-    staged trial kernels switched off) gives the same report and states."""
+    """The per-cell form of the update (every stability test and reflash
+    inside the per-cell code) gives the same report and states."""
     torch = torch_cuda
     name, g, nat = case
-    nat.set_staged_update(False)
+    nat.set_update_mode("per_cell")
     try:
         for it in ("current", "failing"):
             cur = torch.as_tensor(g[it], device="cuda").clone()
@@ -160,7 +161,7 @@ def test_update_state_per_cell_tests(case, torch_cuda):
             else:
                 assert rc == 1
     finally:
-        nat.set_staged_update(True)
+        nat.set_update_mode("staged")
 
 
 def test_update_state_failure_commits_nothing(case, torch_cuda):
@@ -250,9 +251,11 @@ def test_thread_per_cell_mode_parity(reference, torch_cuda):
     oracle.set_history(primary, ps)
     cur = synth.perturb_natural_state(primary, ps, 3, 17, 1.0)
     rc, up, ups, rep = oracle.update_state(cur, ps)
-    c2 = torch.as_tensor(cur, device="cuda")
-    s2 = torch.as_tensor(ps, device="cuda")
-    grc, grep = nat.update_state_with_report(c2, s2)
-    assert grc == rc
-    assert [getattr(grep, f) for f in REPORT_FIELDS] == [getattr(rep, f) for f in REPORT_FIELDS]
-    assert_state(c2.cpu().numpy(), s2.cpu().numpy(), up, ups, "update 200x200x1")
+    for mode in ("per_cell", "staged"):   # one thread per cell at this size, and the staged form
+        nat.set_update_mode(mode)
+        c2 = torch.as_tensor(cur, device="cuda")
+        s2 = torch.as_tensor(ps, device="cuda")
+        grc, grep = nat.update_state_with_report(c2, s2)
+        assert grc == rc, mode
+        assert [getattr(grep, f) for f in REPORT_FIELDS] == [getattr(rep, f) for f in REPORT_FIELDS], mode
+        assert_state(c2.cpu().numpy(), s2.cpu().numpy(), up, ups, f"update 200x200x1 {mode}")
