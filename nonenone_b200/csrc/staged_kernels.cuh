@@ -69,6 +69,7 @@ struct StagedArgs
                               // rounds kMaxRounds.. are the recovery rounds; then full, bound flag,
                               // guard flag, split1 of the current round, continuation queue, rest queue
     unsigned long long *threes;   // three-phase solves: (point << 1) | kind (0 active-set path, 1 recovery 1)
+    unsigned long long *threesLong;   // solves past the lane budget, for the warp kernel (same encoding)
     int *cont;                // points queued for the pressure continuation
     void *anchors;            // AnchorOut<NC>[contCap * 8]
     int64_t contCap;
@@ -87,6 +88,12 @@ constexpr int kCounterCont = kCounterFull + 4;
 constexpr int kCounterRest = kCounterFull + 5;
 constexpr int kCounterThree = kCounterFull + 6;        // queued three-phase solves
 constexpr int kCounterThreeCursor = kCounterFull + 7;  // refill cursor of the three-phase kernel
+constexpr int kCounterThreeLong = kCounterFull + 8;    // solves handed to the warp kernel
+// Steps a lane of the three-phase kernel gives one solve before handing it to
+// the warp kernel.  Most solves end within ~40 steps; the few long ones are
+// long because their robust Rachford-Rice solves fail start after start,
+// which the warp kernel runs on parallel lanes.
+constexpr int kThreeLaneSteps = 48;
 constexpr int kCounterWords = kCounterFull + 12;
 constexpr int kAnchors = 8;
 
@@ -260,6 +267,7 @@ static __global__ void stagedResetSplitKernel(int *counters)
     counters[kCounterSplit1] = 0;
     counters[kCounterThree] = 0;
     counters[kCounterThreeCursor] = 0;
+    counters[kCounterThreeLong] = 0;
 }
 
 // Every queued three-phase solve is a lane running flashThree_ one step at a
@@ -281,6 +289,7 @@ stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
     ThreeLane<NC> L;
     long long point = -1;   // -1 idle, -2 drained
     int kind = 0;
+    int steps = 0;
     unsigned long long evals = 0;
     // a solve takes at most ssi + newton * (1 + 4 nc + 16) + tail steps (a few
     // hundred); the cap only guards against a wait that would never end
@@ -328,6 +337,7 @@ stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                             L.z[c] = st.z[c];
                         threeInit<NC>(s, L, st.threeKg, st.threeKw);
                         point = i;
+                        steps = 0;
                     }
                 }
                 else
@@ -339,7 +349,22 @@ stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
         const bool running = point >= 0;
         if (!__any_sync(0xffffffffu, running))
             break;
-        if (running && threeStep<NC>(s, L))
+        if (!running)
+            continue;
+        if (steps >= kThreeLaneSteps)
+        {
+            // over budget: the warp kernel solves it again from the start
+            const int k = atomicAdd(&a.counters[kCounterThreeLong], 1);
+            if (k >= 0 && k < a.n)
+            {
+                a.threesLong[k] = (static_cast<unsigned long long>(point) << 1) | unsigned(kind);
+                s.err = ERR_NONE;
+                point = -1;
+                continue;
+            }
+        }
+        ++steps;
+        if (threeStep<NC>(s, L))
         {
             DriverState<NC> &st = states[point];
             if (kind == 1)
@@ -351,6 +376,62 @@ stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
         }
     }
     evals += s.evals;
+    warpAddEvals(a.evalCounter, evals);
+}
+
+// The solves the lane kernel handed over: a warp per solve runs flashThree_
+// from its start with the robust Rachford-Rice starts split over the lanes
+// (Solver::rr3Robust's warp path), which is the same solve.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedThreeLongKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
+{
+    const int queued = a.counters[kCounterThreeLong];
+    const int64_t count = queued < a.n ? queued : a.n;
+    const int lane = threadIdx.x & 31;
+    const int64_t warpId = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int nseeds = seedCount<NC>(F);
+    DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+    unsigned long long evals = 0;
+    for (int64_t k = warpId; k < count; k += nwarps)
+    {
+        const unsigned long long task = a.threesLong[k];
+        const int64_t i = int64_t(task >> 1);
+        if (i < 0 || i >= a.n)
+        {
+            if (lane == 0)
+                atomicExch(&a.counters[kCounterBound], 15);
+            continue;
+        }
+        DriverState<NC> &st = states[i];
+        const int kind = int(task & 1u);
+        Solver<NC> s;
+        s.setup(&F, st.sal);
+        s.lane = lane;
+        s.width = 32;
+        if (kind == 1)
+            s.memo = reinterpret_cast<const Rr3Memo<NC> *>(static_cast<const TrialOut<NC> *>(a.trials) +
+                                                            i * 3 * nseeds);
+        double kg[NC], kw[NC];
+        for (int c = 0; c < NC; ++c)
+        {
+            kg[c] = st.threeKg[c];
+            kw[c] = st.threeKw[c];
+        }
+        Result<NC> r;
+        s.flashThree(st.P, st.T, st.z, kg, kw, r);
+        __syncwarp();
+        if (lane == 0)
+        {
+            if (kind == 1)
+                st.lastPhysical = r;
+            else
+                st.current = r;
+            st.err = s.err;
+            evals += s.evals;
+        }
+    }
     warpAddEvals(a.evalCounter, evals);
 }
 
@@ -993,6 +1074,7 @@ size_t stagedScratchBytes(int64_t n, const FluidDev &F)
     add(sizeof(int) * size_t(n));
     add(sizeof(int) * kCounterWords);
     add(sizeof(unsigned long long) * size_t(n));
+    add(sizeof(unsigned long long) * size_t(n));
     const int64_t cap = contCapacity(n);
     add(sizeof(int) * size_t(cap));
     add(sizeof(AnchorOut<NC>) * size_t(cap) * kAnchors);
@@ -1023,6 +1105,7 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
     a.split[1] = reinterpret_cast<int *>(take(sizeof(int) * size_t(n)));
     a.counters = reinterpret_cast<int *>(take(sizeof(int) * kCounterWords));
     a.threes = reinterpret_cast<unsigned long long *>(take(sizeof(unsigned long long) * size_t(n)));
+    a.threesLong = reinterpret_cast<unsigned long long *>(take(sizeof(unsigned long long) * size_t(n)));
     a.contCap = contCapacity(n);
     a.cont = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.contCap)));
     a.anchors = take(sizeof(AnchorOut<NC>) * size_t(a.contCap) * kAnchors);
@@ -1070,6 +1153,7 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         stagedResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round, 0);
         stagedResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round, 1);
         stagedThreeKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a);
+        stagedThreeLongKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
         stagedThreeResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round);
         stagedResetSplitKernel<<<1, 1, 0, st>>>(a.counters);
         if (after("resume", round + 1))
@@ -1078,6 +1162,7 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     stagedRr3MemoKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
     stagedRecoverStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     stagedThreeKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a);
+    stagedThreeLongKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
     stagedRecoverThreeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     if (after("recover", kMaxRounds))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
