@@ -424,7 +424,8 @@ def run_gpu(args):
     step_s = total_ms * 1e-3 / args.steps
     flops = evals_per_batch * f_eos(NC)
     achieved = flops / step_s / 1e12
-    peak = fp64.value if precision != abi.PRECISION_MIXED else fp32.value
+    # NZ_PRECISION_MIXED runs the staged FP64 form (the FP32-SSI form is not built)
+    peak = fp64.value
     status = slots[0]["out"]["status"].cpu().numpy()
     presence = slots[0]["out"]["presence"].cpu().numpy()
     # staged form: start; 8 rounds x (trial, classify, 2 resume, three-phase,
@@ -457,7 +458,7 @@ def run_gpu(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64" if precision == abi.PRECISION_MIXED else "f64",
+            "dtype": "f64",
             "data": "synthetic (seeded mixture, nonenone_b200.synth.flash_points)",
             "config": {"workload": "batched P-T-z flash, 1,048,576 points per batch, nc=3 "
                                    "H2O/CO2/nC10, PR EOS",
@@ -475,7 +476,7 @@ def run_gpu(args):
                     "d2h_bytes_per_step": d2h,
                     "entry_point": "nz_flash_batch on pinned-host-fed device buffers, copies on the "
                                    "batch's stream inside the timed region"},
-            "roofline": {"bound": "fp32" if precision == abi.PRECISION_MIXED else "fp64",
+            "roofline": {"bound": "fp64",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": None,
                          "peak_source": "measured on this GPU by nz_diag_fma_peak (FMA chains); "
