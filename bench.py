@@ -424,15 +424,31 @@ def run_gpu(args):
     step_s = total_ms * 1e-3 / args.steps
     flops = evals_per_batch * f_eos(NC)
     achieved = flops / step_s / 1e12
-    # NZ_PRECISION_MIXED runs the staged FP64 form (the FP32-SSI form is not built)
+    # the FP64 pipe: the mixed form moves only the leading TPD SSI evaluations to FP32
     peak = fp64.value
     status = slots[0]["out"]["status"].cpu().numpy()
     presence = slots[0]["out"]["presence"].cpu().numpy()
-    # staged form: start; 8 rounds x (trial, classify, 2 resume, three-phase,
-    # three-phase resume, reset); RR3 memo, recovery start, three-phase,
-    # recovery-1 accept; 3 recovery rounds x (trial, resume); warp recovery,
-    # 2 continuation-anchor launches, select
-    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 1 + 8 * 7 + 4 + 3 * 2 + 4
+    # staged form: start; 8 rounds x (trial, classify, 2 resume, three-phase lanes,
+    # three-phase warps, three-phase resume, reset); RR3 memo, recovery start,
+    # three-phase lanes and warps, recovery-1 accept; 3 recovery rounds x
+    # (trial, resume); warp recovery, 2 continuation-anchor launches, select
+    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 1 + 8 * 8 + 5 + 3 * 2 + 4
+
+    # the mixed form's distance to the staged FP64 form on the same batch
+    error_vs_fp64 = None
+    if precision == abi.PRECISION_MIXED:
+        s0 = slots[0]
+        f64 = s0["fl"].flash(s0["P"], s0["T"], s0["z"], precision=abi.PRECISION_FP64_STAGED)
+        a = {k: v.cpu().numpy() for k, v in s0["out"].items()}
+        b = {k: v.cpu().numpy() for k, v in f64.items()}
+        same = (a["status"] == b["status"]) & (a["presence"] == b["presence"])
+        ok = same & (b["status"] == 0)
+        error_vs_fp64 = {"points": int(a["status"].size), "label_or_status_mismatch": int((~same).sum())}
+        for key in ("beta", "composition", "saturation", "compressibility", "k_gas_oil", "k_water_oil"):
+            x, y = a[key][..., ok], b[key][..., ok]
+            fin = np.isfinite(y)
+            err = np.abs(x - y)[fin] / np.maximum(1.0, np.abs(y[fin]))
+            error_vs_fp64[key + "_max_rel"] = float(err.max()) if err.size else 0.0
 
     natural = None
     if rank == 0 and not args.no_natural:
@@ -458,7 +474,7 @@ def run_gpu(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f32+f64" if precision == abi.PRECISION_MIXED else "f64",
             "data": "synthetic (seeded mixture, nonenone_b200.synth.flash_points)",
             "config": {"workload": "batched P-T-z flash, 1,048,576 points per batch, nc=3 "
                                    "H2O/CO2/nC10, PR EOS",
@@ -487,6 +503,7 @@ def run_gpu(args):
                                              "F_eos(nc) = 2 nc^2 + 13 nc + 50",
                          "kernel": "flash pipeline (all kernels of one batch)"},
             "gpu_launches": args.steps * kernels_per_batch,
+            "error_vs_fp64": error_vs_fp64,
             "clocks": clocks.summary(),
             "fp32_fma_peak_tflops": fp32.value,
             "cpu_baseline": cpu,

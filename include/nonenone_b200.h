@@ -182,7 +182,8 @@ typedef struct nz_flash_out {
 } nz_flash_out;
 
 #define NZ_PRECISION_FP64 0         /* plain FP64 form: one thread runs one point's whole flash */
-#define NZ_PRECISION_MIXED 1        /* reserved for the FP32-SSI form; runs the staged FP64 form */
+#define NZ_PRECISION_MIXED 1        /* staged; leading SSI steps of the TPD trials with FP32 mixing and
+                                       ln phi (FP64 root), every trial finished in FP64 */
 #define NZ_PRECISION_FP64_STAGED 2  /* staged, every TPD trial in FP64 exactly as the plain form */
 
 int nz_flash_batch(nz_ctx* ctx, int64_t n, const double* pressure,

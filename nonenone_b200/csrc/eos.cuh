@@ -375,6 +375,52 @@ NZ_HDI bool fugacityCoefficients(const double *x, const MixParams<NC> &p,
     return true;
 }
 
+// ln phi_i of one phase with the mixing sums and the fugacity expression in
+// FP32 and the cubic root chosen in FP64 (the mixed-precision form's
+// successive-substitution evaluations).  False when the FP32 evaluation has no
+// admissible root or a non-finite term; the caller then evaluates in FP64.
+template <int NC>
+NZ_HDI bool lnPhiMixed(const double *x, const MixParams<NC> &p, double m1, double m2, bool vapour,
+                       double *lnphi)
+{
+    float xf[NC], S[NC];
+    float A = 0.0f, B = 0.0f;
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+        xf[i] = float(x[i]);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+    {
+        float si = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NC; ++j)
+            si += xf[j] * float(p.A[i][j]);
+        S[i] = si;
+        B += xf[i] * float(p.B[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+        A += xf[i] * S[i];
+    if (!(B > 0.0f) || !(A > 0.0f))
+        return false;
+    const double Z = selectCubicRoot(double(A), double(B), m1, m2, vapour);
+    if (!isfinite(Z) || !(Z - double(B) > 0.0))
+        return false;
+    const float z = float(Z), m1f = float(m1), m2f = float(m2);
+    const float commonA = -logf(z - B);
+    const float commonB = logf((z + m2f * B) / (z + m1f * B)) * A / ((m1f - m2f) * B);
+    const float commonC = (z - 1.0f) / B;
+    bool ok = isfinite(commonA) && isfinite(commonB) && isfinite(commonC);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+    {
+        const float l = commonA + commonB * (2.0f * S[i] / A - float(p.B[i]) / B) + float(p.B[i]) * commonC;
+        ok = ok && isfinite(l);
+        lnphi[i] = double(l);
+    }
+    return ok;
+}
+
 // molarDensity without volume translation (cubic_eos.hpp:511-523)
 NZ_HDI double molarDensity(double P, double T, double Z)
 {

@@ -95,6 +95,7 @@ struct StabilityResidual
     double x[NC];
     double residual[NC];
     double phi[NC];
+    double lnphi[NC];   // set by the mixed-precision evaluation only
 };
 
 template <int NC>
@@ -322,6 +323,7 @@ struct Solver
     const Rr3Memo<NC> *memo;   // optional precomputed rr3Robust answer
     StabilityMemo<NC> *stabMemo;   // optional precomputed stability test
     const FlashMemo<NC> *flashMemo;   // optional precomputed top-level flash
+    bool mixed;                    // mixed-precision successive substitution in the TPD trials
 
     NZ_HD void setup(const FluidDev *fluid, double s)
     {
@@ -339,6 +341,7 @@ struct Solver
         memo = nullptr;
         stabMemo = nullptr;
         flashMemo = nullptr;
+        mixed = false;
     }
 
     NZ_HD const FlashOpts &O() const { return F->opt; }
@@ -1493,6 +1496,57 @@ struct Solver
             s.norm = smax(s.norm, fabs(s.residual[i]));
         }
         s.valid = isfinite(s.norm);
+    }
+
+    // evaluateStabilityResidual_ with ln phi from lnPhiMixed (FP32 mixing and
+    // fugacity expression, FP64 root; the normalisation of W stays FP64).
+    // False when that evaluation fails or the fluid is CPA: the caller then
+    // evaluates in FP64.
+    NZ_HDN bool stabilityResidualMixed(int candidate, double P, double T, const double *logRef,
+                                       const double *logW, StabilityResidual<NC> &s)
+    {
+        if (F->eosModel == EOS_CPA)
+            return false;
+        s.valid = false;
+        double maxLogW = logW[0];
+#pragma unroll
+        for (int i = 1; i < NC; ++i)
+            if (maxLogW < logW[i])
+                maxLogW = logW[i];
+        if (!isfinite(maxLogW))
+            return false;
+        double scaledSum = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double v = exp(logW[i] - maxLogW);
+            if (!(v > 0.0) || !isfinite(v))
+                return false;
+            s.x[i] = v;
+            scaledSum += v;
+        }
+        if (!(scaledSum > 0.0) || !isfinite(scaledSum))
+            return false;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            s.x[i] /= scaledSum;
+        const double logSum = maxLogW + log(scaledSum);
+        s.sum = logSum > 709.782712893384 ? nzInf() : exp(logSum);
+        const int role = thermodynamicRole(candidate);
+        ensureCache(P, T);
+        const MixParams<NC> &p = (role == WATER && sw()) ? aq : nonAq;
+        if (!lnPhiMixed<NC>(s.x, p, F->m1, F->m2, role == GAS, s.lnphi))
+            return false;
+        ++evals;
+        s.norm = 0.0;
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            s.residual[i] = logW[i] + s.lnphi[i] - logRef[i];
+            s.norm = smax(s.norm, fabs(s.residual[i]));
+        }
+        s.valid = isfinite(s.norm);
+        return s.valid;
     }
 
     // finalizeStabilityTrial_ (stability.inc:206-223)

@@ -21,21 +21,21 @@ template <int NC>
 int launchStaged(nz_ctx *ctx, int64_t n, const double *P, const double *T, const double *z,
                  const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st)
 {
-    (void)mixed;
     const size_t bytes = stagedScratchBytes<NC>(n, ctx->fluid);
     const int rc = ctx->ensureScratch(bytes);
     if (rc != 0)
         return rc;
-    return stagedLaunch<NC>(ctx->fluid, ctx->scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st);
+    return stagedLaunch<NC>(ctx->fluid, ctx->scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st,
+                            mixed);
 }
 template <int NC>
 int launchStagedInto(nz_ctx *ctx, void *scratch, size_t capacity, int64_t n, const double *P, const double *T,
                      const double *z, const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st)
 {
-    (void)mixed;
     if (stagedScratchBytes<NC>(n, ctx->fluid) > capacity)
         return setError(NZ_ERR_ARGUMENT, "staged flash: work space too small");
-    return stagedLaunch<NC>(ctx->fluid, scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st);
+    return stagedLaunch<NC>(ctx->fluid, scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st,
+                            mixed);
 }
 template <int NC>
 size_t stagedScratchBytesNc(int64_t n, const FluidDev &F)

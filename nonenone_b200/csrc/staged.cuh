@@ -575,6 +575,7 @@ struct Driver
 // One lane = one TPD trial of stabilityTrial_ (stability.inc:225-355), driven
 // one EOS evaluation per step so every lane of a warp executes the EOS code
 // together whatever phase of the trial it is in.
+constexpr double kMixedSsiHandover = 1.0e-5;   // mixed form: FP32 residual below which FP64 SSI takes over
 constexpr int TM_SSI = 0;        // leading SSI steps
 constexpr int TM_NEWTON = 1;     // Newton base evaluation
 constexpr int TM_FD = 2;         // finite-difference column evaluation
@@ -589,6 +590,7 @@ struct TrialLane
     int newtonIt;
     int col;           // FD column / line-search step
     int candidate;
+    bool fp64Ssi;      // mixed form: the leading SSI steps have gone over to FP64
     double P, T;
     double logW[NC];
     double logRef[NC];
@@ -614,6 +616,7 @@ NZ_HD void trialInit(Solver<NC> &s, TrialLane<NC> &L, const double *seedIn)
         L.logW[i] = log(smax(seed[i], s.O().floor));
     L.it = 0;
     L.newtonIt = 0;
+    L.fp64Ssi = false;
     const int ssiSteps = imin(s.O().maxStability, imax(s.O().stabilitySsi, 0));
     L.mode = ssiSteps > 0 ? TM_SSI : (s.O().stabilityNewton > 0 ? TM_NEWTON : TM_TAIL);
 }
@@ -645,9 +648,33 @@ NZ_HD int trialStep(Solver<NC> &s, TrialLane<NC> &L, TrialOut<NC> &out)
 {
     StabilityResidual<NC> r;
     const bool probing = L.mode == TM_FD || L.mode == TM_LINE;
-    s.stabilityResidual(L.candidate, L.P, L.T, L.logRef, probing ? L.probe : L.logW, r);
     const FlashOpts &O = s.O();
     const int ssiSteps = imin(O.maxStability, imax(O.stabilitySsi, 0));
+    // Mixed form: the leading SSI steps evaluate ln phi with FP32 mixing (FP64
+    // root) and never end a trial.  Once the FP32 residual is small the rest of
+    // the leading steps run in FP64 (where a trial may converge, as in the
+    // FP64 form); the Newton steps and the SSI tail are FP64 throughout.
+    if (L.mode == TM_SSI && s.mixed && !L.fp64Ssi &&
+        s.stabilityResidualMixed(L.candidate, L.P, L.T, L.logRef, L.logW, r))
+    {
+        for (int i = 0; i < NC; ++i)
+            L.logW[i] = L.logRef[i] - r.lnphi[i];
+        ++L.it;
+        if (L.it >= ssiSteps)
+        {
+            if (O.stabilityNewton > 0)
+            {
+                L.mode = TM_NEWTON;
+                L.it = 0;
+            }
+            else if (!trialEnterTail(s, L))
+                return -1;
+        }
+        else if (r.norm < kMixedSsiHandover)
+            L.fp64Ssi = true;
+        return 0;
+    }
+    s.stabilityResidual(L.candidate, L.P, L.T, L.logRef, probing ? L.probe : L.logW, r);
     switch (L.mode)
     {
     case TM_SSI:

@@ -74,6 +74,7 @@ struct StagedArgs
     void *anchors;            // AnchorOut<NC>[contCap * 8]
     int64_t contCap;
     unsigned long long *evalCounter;
+    int mixed;   // TPD trials: mixed-precision leading SSI steps
 };
 
 // Per-round counters for the active-set rounds and the recovery rounds, then
@@ -517,6 +518,7 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                     const DriverState<NC> &st = states[bad ? 0 : point];
                     evals += s.evals;
                     s.setup(&F, st.sal);
+                    s.mixed = a.mixed != 0;
                     L.P = st.P;
                     L.T = st.T;
                     L.candidate = cand;
@@ -1117,9 +1119,10 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
 template <int NC>
 int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
                  const double *z, const double *sal, const nz_flash_out &out,
-                 unsigned long long *evalCounter, int smCount, cudaStream_t st)
+                 unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed = false)
 {
     StagedArgs a = stagedCarve<NC>(scratch, n, F);
+    a.mixed = mixed ? 1 : 0;
     a.P = P;
     a.T = T;
     a.z = z;

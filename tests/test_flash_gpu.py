@@ -211,6 +211,30 @@ def test_staged_fp64_matches_golden(torch_cuda, golden, name, fluid_args):
     compare_flash(out, g)
 
 
+@pytest.mark.parametrize("name,fluid_args", [
+    ("flash_pr_nc3.npz", dict()),
+    ("flash_sw_nc3.npz", dict(eos_model=abi.EOS_SW)),
+    ("flash_pr_nc6.npz", dict(names=SIX_COMPONENT)),
+    ("flash_continuation_pr_nc3.npz", dict()),
+])
+def test_mixed_precision_matches_golden(torch_cuda, golden, name, fluid_args):
+    """The mixed-precision form (FP32 mixing / ln phi in the leading SSI steps of
+    the TPD trials, FP64 root, trials finished in FP64) against the reference
+    with the FP64 form's tolerances, and against the staged FP64 form."""
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    g = golden(name)
+    fl = CubicThreePhaseFlash(_fluid(fluid_args))
+    mixed = _np(fl.flash(g["P"], g["T"], g["z"], salinity=g.get("salinity"), precision=abi.PRECISION_MIXED))
+    compare_flash(mixed, g)
+    fp64 = _np(fl.flash(g["P"], g["T"], g["z"], salinity=g.get("salinity"), precision=abi.PRECISION_FP64_STAGED))
+    same = (mixed["status"] == fp64["status"]) & (mixed["presence"] == fp64["presence"])
+    assert (~same & ~_near_boundary(g)).sum() == 0
+    ok = same & (fp64["status"] == abi.FLASH_CONVERGED)
+    for key in ("beta", "composition"):
+        err = np.abs(mixed[key][..., ok] - fp64[key][..., ok]) / np.maximum(1.0, np.abs(fp64[key][..., ok]))
+        assert err.max() <= VALUE_TOL, (key, err.max())
+
+
 def test_staged_fp64_equals_plain_fp64(torch_cuda, golden):
     """Staging changes the schedule, not the arithmetic: same labels, values to rounding."""
     from nonenone_b200.flash import CubicThreePhaseFlash
