@@ -212,8 +212,11 @@ int nz_flash_eos_eval_count(nz_ctx* ctx, uint64_t* count);
  * static device array of NZ_NOALLOC_SCRATCH_BYTES that every GPU which loads
  * this library holds until the process exits; it calls no cudaMalloc /
  * cudaFree.  Batches whose work space would exceed the array are rejected
- * with NZ_ERR_ARGUMENT (at most 14,026 points for nc = 3, 7,727 for nc = 6,
- * 5,704 for nc = 8).  The first call on a
+ * with NZ_ERR_ARGUMENT.  The limit depends on the fluid (its component count
+ * and whether it has a water component, which adds a stability seed); the
+ * error message states the exact limit for the context's fluid.  For fluids
+ * with a water component it is 14,026 points for nc = 3, 7,727 for nc = 6 and
+ * 5,704 for nc = 8.  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress) and
  * should therefore come before any stream capture.  All calls share the one
  * array and the context's evaluation counter: calls that overlap on the GPU

@@ -85,15 +85,18 @@ def build(verbose: bool = False, nc_list=NC_LIST, jobs: int | None = None) -> st
     return LIB
 
 
-def build_oracle(verbose: bool = False) -> None:
+def build_oracle(verbose: bool = False, reference: str | None = None) -> None:
     """Compile the oracle (test infrastructure): the C restatement always, and
-    the reference's own code when its source tree is present here."""
+    the reference's own code when the path of its source tree is given
+    (`reference`, else the NZ_REFERENCE environment variable) and exists."""
     oracle = os.path.join(ROOT, "oracle")
     targets = ["restatement"]
-    ref_root = os.environ.get("NZ_REFERENCE", "/root/reference")
-    if os.path.isdir(ref_root):
+    ref_root = reference or os.environ.get("NZ_REFERENCE")
+    args = []
+    if ref_root and os.path.isdir(ref_root):
         targets.append("ref")
-    r = subprocess.run(["make", "-C", oracle, f"REFERENCE={ref_root}", *targets],
+        args.append(f"REFERENCE={ref_root}")
+    r = subprocess.run(["make", "-C", oracle, *args, *targets],
                        capture_output=not verbose, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{(r.stderr or '')[-4000:]}")
@@ -104,11 +107,13 @@ def main():
     ap.add_argument("-v", "--verbose", action="store_true")
     ap.add_argument("--nc", default=",".join(map(str, NC_LIST)))
     ap.add_argument("--oracle", action="store_true")
+    ap.add_argument("--reference", default=None,
+                    help="source tree of the reference, for the oracle's compiled reference")
     a = ap.parse_args()
     nc_list = tuple(int(x) for x in a.nc.split(","))
     print(build(a.verbose, nc_list))
     if a.oracle:
-        build_oracle(a.verbose)
+        build_oracle(a.verbose, a.reference)
 
 
 if __name__ == "__main__":

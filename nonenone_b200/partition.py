@@ -191,33 +191,42 @@ def combine_reports(dom: RankDomain, reports: List[abi.Report]) -> abi.Report:
 
 class TorchComm:
     """Point-to-point halo exchange and report gathering over torch.distributed
-    (NCCL between GPUs, gloo on CPU).  Arrays travel as torch tensors."""
+    (NCCL between GPUs, gloo on CPU).  Arrays travel as torch tensors.
+
+    ``exchange`` issues every send and receive of one halo exchange as a single
+    ``dist.batch_isend_irecv`` call: NCCL needs the send to and the receive
+    from the same peer in one group, or two ranks that exchange with each other
+    can both block once a message exceeds the eager buffer.  Receive buffers
+    take the dtype of the array being exchanged (float64 primaries and phase
+    states, integer labels alike)."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
-        self._pending = []
 
-    def send(self, peer: int, rows):
+    def exchange(self, dom: "RankDomain", local) -> None:
         import torch
-        t = rows if isinstance(rows, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(rows))
-        t = t.contiguous()
-        self._pending.append((self.dist.isend(t, peer, group=self.group), t))
-
-    def recv(self, peer: int, like, n: int):
-        import torch
-        if isinstance(like, torch.Tensor):
-            buf = torch.empty((n,) + tuple(like.shape[1:]), dtype=like.dtype, device=like.device)
-        else:
-            buf = torch.empty((n,) + tuple(like.shape[1:]), dtype=torch.float64)
-        self.dist.irecv(buf, peer, group=self.group).wait()
-        return buf if isinstance(like, torch.Tensor) else buf.numpy()
-
-    def flush(self):
-        for work, _ in self._pending:
-            work.wait()
-        self._pending = []
+        is_tensor = isinstance(local, torch.Tensor)
+        ops, recvs, keep = [], [], []
+        for peer, idx in sorted(dom.send_to.items()):
+            rows = local[_index(local, idx)]
+            t = rows.contiguous() if is_tensor else torch.from_numpy(np.ascontiguousarray(rows))
+            keep.append(t)
+            ops.append(self.dist.P2POp(self.dist.isend, t, peer, group=self.group))
+        for peer, idx in sorted(dom.recv_from.items()):
+            shape = (len(idx),) + tuple(local.shape[1:])
+            if is_tensor:
+                buf = torch.empty(shape, dtype=local.dtype, device=local.device)
+            else:
+                buf = torch.from_numpy(np.empty(shape, dtype=np.asarray(local).dtype))
+            recvs.append((idx, buf))
+            ops.append(self.dist.P2POp(self.dist.irecv, buf, peer, group=self.group))
+        if ops:
+            for work in self.dist.batch_isend_irecv(ops):
+                work.wait()
+        for idx, buf in recvs:
+            local[_index(local, idx)] = buf if is_tensor else buf.numpy()
 
     def gather_reports(self, rep: abi.Report) -> List[abi.Report]:
         fields = [f for f, _ in abi.Report._fields_]
@@ -239,8 +248,8 @@ class DistributedNatural:
     `make(grid)` builds the rank's compute object on a local grid; it must offer
     ``set_history(p, s)``, ``residual(p, s)``, ``jacobian(p, s)``, ``pattern()``
     and ``update(p, s) -> (rc, p_new, s_new, report)`` (arrays cell-major, the
-    Vec layouts).  `comm` offers ``send``, ``recv``, ``flush`` and
-    ``gather_reports`` (``TorchComm``)."""
+    Vec layouts).  `comm` offers ``exchange(dom, arr)`` (``TorchComm``) or
+    ``send``, ``recv`` and ``flush``, and ``gather_reports``."""
 
     def __init__(self, grid, nranks: int, rank: int, make: Callable, comm):
         self.dom = RankDomain(grid, nranks, rank)
@@ -251,6 +260,9 @@ class DistributedNatural:
         self.owned_blocks = self.dom.owned_rows(rp)
 
     def _exchange(self, arr):
+        if hasattr(self.comm, "exchange"):
+            self.comm.exchange(self.dom, arr)
+            return
         exchange_halo(self.dom, arr, self.comm.send, lambda peer, n: self.comm.recv(peer, arr, n))
         self.comm.flush()
 

@@ -124,7 +124,13 @@ def _rank_main(rank, world, port, out_dir):
         J = dn.jacobian(cp, cs)
         rc, up, ups, rep = dn.update_state(g["current"][own], g["phase_state"][own])
         frc, fp, fs, frep = dn.update_state(g["failing"][own], g["phase_state"][own])
+        # an integer array (phase labels) through the same batched exchange
+        lab = np.full((nl, 2), -1, np.int32)
+        lab[dn.dom.owned_local, 0] = 7 * own + 3
+        lab[dn.dom.owned_local, 1] = own % 5
+        dn.comm.exchange(dn.dom, lab)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), owned=own, F=F, J=J, rc=rc, up=up, ups=ups,
+                 lab=lab, cells=dn.dom.cells,
                  rep=np.array([getattr(rep, f) for f in REPORT_FIELDS]), frc=frc, fp=fp, fs=fs,
                  frep=np.array([getattr(frep, f) for f in REPORT_FIELDS]))
     finally:
@@ -161,3 +167,7 @@ def test_partitioned_natural_equals_single_domain(world, tmp_path):
         assert int(d["frc"]) == 1
         assert np.array_equal(d["fp"], g["failing"][own]) and np.array_equal(d["fs"], g["phase_state"][own])
         assert np.array_equal(d["frep"], g["failing_report"]), r
+        # every local row, halo included, holds its owner's integer labels
+        assert d["lab"].dtype == np.int32
+        assert np.array_equal(d["lab"][:, 0], 7 * d["cells"] + 3), r
+        assert np.array_equal(d["lab"][:, 1], d["cells"] % 5), r
