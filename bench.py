@@ -301,9 +301,54 @@ def run_reference(args):
     return 0
 
 
-def run_gpu(args):
-    import ctypes as C
+FORMS = ("fp64", "fp64_staged", "mixed")
 
+
+def staged_launches(precision_name: str) -> int:
+    """Kernels one batch launches: the plain FP64 form one; the staged forms
+    start, 8 rounds x 8, recovery 1 (5), recovery 2 (3 x 2), the full solver,
+    2 continuation-anchor launches, select and check (+ the polish of the
+    mixed form)."""
+    if precision_name == "fp64":
+        return 1
+    return 1 + 8 * 8 + 5 + 3 * 2 + 1 + 2 + 1 + 1 + (1 if precision_name == "mixed" else 0)
+
+
+def form_error(out, ref_out):
+    """Label / status differences and largest relative value differences of a
+    flash answer against another on the same batch (both device dicts)."""
+    a = {k: v.cpu().numpy() for k, v in out.items()}
+    b = {k: v.cpu().numpy() for k, v in ref_out.items()}
+    same = (a["status"] == b["status"]) & (a["presence"] == b["presence"])
+    ok = same & (b["status"] == 0)
+    err = {"points": int(a["status"].size), "label_or_status_mismatch": int((~same).sum())}
+    present = np.stack([(b["presence"] >> p) & 1 for p in range(3)]).astype(bool) & ok
+    for key in ("beta", "composition", "saturation", "compressibility", "k_gas_oil", "k_water_oil"):
+        x, y = a[key], b[key]
+        if key in ("saturation", "compressibility"):
+            x, y = x[present], y[present]
+        else:
+            x, y = x[..., ok], y[..., ok]
+        fin = np.isfinite(y)
+        e = np.abs(x - y)[fin] / np.maximum(1.0, np.abs(y[fin]))
+        err[key + "_max_rel"] = float(e.max()) if e.size else 0.0
+    return err
+
+
+def residual_summary(eos, P, T, out, salinity=None):
+    import torch
+    from nonenone_b200.flash import fugacity_residual
+    r = fugacity_residual(eos, P, T, out, salinity=salinity)
+    fin = r[torch.isfinite(r)]
+    if not fin.numel():
+        return {"fugacity_residual_max": None}
+    return {"fugacity_residual_max": float(fin.max()),
+            "fugacity_residual_p99": float(torch.quantile(fin[:1 << 24], 0.99)),
+            "fugacity_residual_above_1e-10": int((fin > 1e-10).sum()),
+            "multiphase_points": int(fin.numel())}
+
+
+def run_gpu(args):
     import torch
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
@@ -314,54 +359,66 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from nonenone_b200 import abi, synth
     from nonenone_b200.fluids import make_fluid
-    from nonenone_b200.flash import CubicThreePhaseFlash
+    from nonenone_b200.flash import CubicEquationOfState, CubicThreePhaseFlash
     from nonenone_b200.lib import load
 
+    prec_of = {"fp64": abi.PRECISION_FP64, "fp64_staged": abi.PRECISION_FP64_STAGED,
+               "mixed": abi.PRECISION_MIXED}
+    headline = args.precision
+    precision = prec_of[headline]
     fluid = make_fluid()
-    precision = {"fp64": abi.PRECISION_FP64, "fp64_staged": abi.PRECISION_FP64_STAGED,
-                 "mixed": abi.PRECISION_MIXED}[args.precision]
     M = max(1, args.inflight)
     dev = torch.device("cuda", local)
-    # M independent batches in flight: one context (work space), stream,
-    # input set and output set each.  Step k flashes batch k % M.
+    main = torch.cuda.current_stream()
+
+    # the benchmark batch: the label mixture plus the 5 % near-boundary slice,
+    # bisected once with this GPU's own staged FP64 labels (untimed) and shared
+    # by the batches in flight
+    labeler = CubicThreePhaseFlash(fluid, device=local)
+
+    def labels(P, T, z, s):
+        return labeler.flash(P, T, z, salinity=s, precision=abi.PRECISION_FP64_STAGED)["presence"].cpu().numpy()
+
+    nb = int(round(synth.BOUNDARY_FRACTION * N_POINTS))
+    boundary = synth.boundary_points(nb, labels, seed=7919 + rank)
     slots = []
     for m in range(M):
         fl = CubicThreePhaseFlash(fluid, device=local)
-        P, T, z = synth.flash_points(N_POINTS, seed=1 + 1000 * rank + m)
+        P, T, z = synth.benchmark_points(N_POINTS, boundary, seed=1 + 1000 * rank + m)
         slots.append(dict(
             fl=fl, stream=torch.cuda.Stream(device=dev),
             P=torch.tensor(P, device=dev), T=torch.tensor(T, device=dev),
             z=torch.tensor(z, device=dev), out=fl.allocate(N_POINTS), host=(P, T, z)))
-    main = torch.cuda.current_stream()
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    def launch(k):
-        sl = slots[k % M]
-        sl["fl"].flash(sl["P"], sl["T"], sl["z"], out=sl["out"], precision=precision,
-                       stream=sl["stream"])
-
-    def run_steps(nsteps, e0, e1):
+    def run_steps(nsteps, prec, e0, e1, inflight=M):
         e0.record(main)
-        for sl in slots:
+        for sl in slots[:inflight]:
             sl["stream"].wait_event(e0)
         for k in range(nsteps):
-            launch(k)
-        for sl in slots:
+            sl = slots[k % inflight]
+            sl["fl"].flash(sl["P"], sl["T"], sl["z"], out=sl["out"], precision=prec, stream=sl["stream"])
+        for sl in slots[:inflight]:
             ev = torch.cuda.Event()
             ev.record(sl["stream"])
             main.wait_event(ev)
         e1.record(main)
 
+    def timed_rate(prec, nsteps, inflight):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        run_steps(nsteps, prec, a, b, inflight)
+        torch.cuda.synchronize()
+        return N_POINTS * nsteps / (a.elapsed_time(b) * 1e-3)
+
     w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    run_steps(max(args.warmup, 1), w0, w1)
+    run_steps(max(args.warmup, 1), precision, w0, w1)
     barrier()
-    # per-batch latency of one isolated batch (p50 / p99 over a few repeats)
     lat = []
-    for _ in range(3):
+    for _ in range(args.latency_reps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(main)
         slots[0]["fl"].flash(slots[0]["P"], slots[0]["T"], slots[0]["z"], out=slots[0]["out"],
@@ -374,7 +431,7 @@ def run_gpu(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         barrier()
-        run_steps(args.steps, e0, e1)
+        run_steps(args.steps, precision, e0, e1)
         barrier()
     total_ms = e0.elapsed_time(e1)
     if dist is not None:
@@ -382,6 +439,7 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = N_POINTS * world * args.steps / (total_ms * 1e-3)
+    self_check = slots[0]["fl"].self_check() if precision != abi.PRECISION_FP64 else (0, 0)
 
     # --- e2e: pinned host inputs -> public entry point -> pinned host results ----
     for sl in slots:
@@ -427,39 +485,67 @@ def run_gpu(args):
         e2e_s = float(t.item())
     e2e_value = N_POINTS * world * e2e_steps / e2e_s
 
+    # --- the other forms on the same batches, accuracy of each -------------------
+    forms = None
+    sw_half = None
+    if rank == 0 and not args.no_forms:
+        eos = CubicEquationOfState(fluid, device=local)
+        s0 = slots[0]
+        ref_out = s0["fl"].flash(s0["P"], s0["T"], s0["z"], precision=abi.PRECISION_FP64_STAGED)
+        torch.cuda.synchronize()
+        forms = {}
+        for name in FORMS:
+            pr = prec_of[name]
+            if name == headline:
+                rate = value / world
+            else:
+                inflight = min(2, M)
+                timed_rate(pr, inflight, inflight)   # warm-up of the form
+                rate = timed_rate(pr, inflight, inflight)
+            o = s0["fl"].flash(s0["P"], s0["T"], s0["z"], precision=pr)
+            entry = {"flashes_per_s": rate, **residual_summary(eos, s0["P"], s0["T"], o)}
+            if name != "fp64_staged":
+                entry["error_vs_fp64_staged"] = form_error(o, ref_out)
+            forms[name] = entry
+        base = forms["fp64"]["flashes_per_s"]
+        for name in FORMS:
+            forms[name]["vs_plain_fp64"] = forms[name]["flashes_per_s"] / base
+        # the Soreide-Whitson half: the same mixture with salinity ~ U[0,2] mol/kg
+        swf = make_fluid(eos_model=abi.EOS_SW)
+        swl = CubicThreePhaseFlash(swf, device=local)
+        swe = CubicEquationOfState(swf, device=local)
+        Pw, Tw, zw, sal = synth.flash_points(N_POINTS, seed=2 + 1000 * rank, salinity=True)
+        dPw, dTw, dzw, dsw = (torch.tensor(x, device=dev) for x in (Pw, Tw, zw, sal))
+        sw_half = {"workload": "1,048,576 points of the label mixture, Soreide-Whitson, salinity ~ U[0,2]"}
+        sw_ref = None
+        for name in ("fp64_staged", "mixed"):
+            pr = prec_of[name]
+            outw = swl.allocate(N_POINTS)
+            swl.flash(dPw, dTw, dzw, salinity=dsw, precision=pr, out=outw)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(main)
+            swl.flash(dPw, dTw, dzw, salinity=dsw, precision=pr, out=outw)
+            b.record(main)
+            torch.cuda.synchronize()
+            sw_half[name] = {"flashes_per_s_one_batch": N_POINTS / (a.elapsed_time(b) * 1e-3),
+                             **residual_summary(swe, dPw, dTw, outw, salinity=dsw)}
+            if sw_ref is None:
+                sw_ref = {k: v.clone() for k, v in outw.items()}
+            else:
+                sw_half[name]["error_vs_fp64_staged"] = form_error(outw, sw_ref)
+
     # --- roofline ---------------------------------------------------------------
     lib = load()
+    import ctypes as C
     fp64 = C.c_double()
     fp32 = C.c_double()
     lib.nz_diag_fma_peak(local, C.byref(fp64), C.byref(fp32))
     step_s = total_ms * 1e-3 / args.steps
     flops = evals_per_batch * f_eos(NC)
     achieved = flops / step_s / 1e12
-    # the FP64 pipe: the mixed form moves only the leading TPD SSI evaluations to FP32
     peak = fp64.value
     status = slots[0]["out"]["status"].cpu().numpy()
     presence = slots[0]["out"]["presence"].cpu().numpy()
-    # staged form: start; 8 rounds x (trial, classify, 2 resume, three-phase lanes,
-    # three-phase warps, three-phase resume, reset); RR3 memo, recovery start,
-    # three-phase lanes and warps, recovery-1 accept; 3 recovery rounds x
-    # (trial, resume); warp recovery, 2 continuation-anchor launches, select
-    kernels_per_batch = 1 if precision == abi.PRECISION_FP64 else 1 + 8 * 8 + 5 + 3 * 2 + 4
-
-    # the mixed form's distance to the staged FP64 form on the same batch
-    error_vs_fp64 = None
-    if precision == abi.PRECISION_MIXED:
-        s0 = slots[0]
-        f64 = s0["fl"].flash(s0["P"], s0["T"], s0["z"], precision=abi.PRECISION_FP64_STAGED)
-        a = {k: v.cpu().numpy() for k, v in s0["out"].items()}
-        b = {k: v.cpu().numpy() for k, v in f64.items()}
-        same = (a["status"] == b["status"]) & (a["presence"] == b["presence"])
-        ok = same & (b["status"] == 0)
-        error_vs_fp64 = {"points": int(a["status"].size), "label_or_status_mismatch": int((~same).sum())}
-        for key in ("beta", "composition", "saturation", "compressibility", "k_gas_oil", "k_water_oil"):
-            x, y = a[key][..., ok], b[key][..., ok]
-            fin = np.isfinite(y)
-            err = np.abs(x - y)[fin] / np.maximum(1.0, np.abs(y[fin]))
-            error_vs_fp64[key + "_max_rel"] = float(err.max()) if err.size else 0.0
 
     natural = None
     if rank == 0 and not args.no_natural:
@@ -486,19 +572,20 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if precision == abi.PRECISION_MIXED else "f64",
-            "data": "synthetic (seeded mixture, nonenone_b200.synth.flash_points)",
-            "config": {"workload": "batched P-T-z flash, 1,048,576 points per batch, nc=3 "
-                                   "H2O/CO2/nC10, PR EOS",
+            "data": "synthetic (seeded: nonenone_b200.synth label mixture + 5 % near-boundary slice)",
+            "config": {"workload": WORKLOAD,
                        "points_per_batch": N_POINTS, "eos": "PR", "nc": NC,
-                       "precision": args.precision, "batches_in_flight": M,
+                       "precision": headline, "batches_in_flight": M,
+                       "near_boundary_points": nb,
                        "l2": f"not flushed: {M} distinct input sets of 42 MB and output sets of "
                              f"{d2h / 1e6:.0f} MB per batch in flight exceed the 126 MB L2",
                        "label_mix": {"single": float(np.isin(presence, [1, 2, 4]).mean()),
                                      "two": float(np.isin(presence, [3, 5, 6]).mean()),
                                      "three": float((presence == 7).mean()),
                                      "failed": float((status != 0).mean())}},
-            "latency_ms": {"p50": lat_sorted[len(lat_sorted) // 2], "max_of_3": lat_sorted[-1],
-                           "what": "one isolated 1,048,576-point batch, CUDA events"},
+            "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)),
+                           "p99": float(np.percentile(lat_sorted, 99)), "samples": len(lat_sorted),
+                           "what": "one isolated 1,048,576-point batch of the headline form, CUDA events"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "entry_point": "nz_flash_batch on pinned-host-fed device buffers, copies on the "
@@ -513,8 +600,10 @@ def run_gpu(args):
                          "flops_convention": "executed single-phase EOS evaluations x F_eos(nc), "
                                              "F_eos(nc) = 2 nc^2 + 13 nc + 50",
                          "kernel": "flash pipeline (all kernels of one batch)"},
-            "gpu_launches": args.steps * kernels_per_batch,
-            "error_vs_fp64": error_vs_fp64,
+            "gpu_launches": args.steps * staged_launches(headline),
+            "self_check": {"queue_bound": self_check[0], "spin_guard": self_check[1]},
+            "forms": forms,
+            "sw_half": sw_half,
             "clocks": clocks.summary(),
             "fp32_fma_peak_tflops": fp32.value,
             "cpu_baseline": cpu,
@@ -533,7 +622,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nz", choices=["nz", "reference"])
-    ap.add_argument("--precision", default="fp64_staged", choices=["fp64", "fp64_staged", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "fp64_staged", "mixed"],
+                    help="headline form (the others are measured beside it unless --no-forms)")
+    ap.add_argument("--latency-reps", type=int, default=8)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the other precision forms and the Soreide-Whitson half")
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="workload size of the reference arm (the benchmark's is 1,048,576)")

@@ -46,6 +46,7 @@ extern "C" {
 #define NZ_ERR_CUDA (-2)
 #define NZ_ERR_UNSUPPORTED (-3)
 #define NZ_ERR_ALLOC (-4)
+#define NZ_ERR_SELFCHECK (-5)     /* a device self-check (queue bound, spin guard) stopped a batch */
 
 /* per-point flash status (nz_flash_out.status) */
 #define NZ_FLASH_CONVERGED 0
@@ -53,6 +54,8 @@ extern "C" {
 #define NZ_FLASH_BAD_INPUT 2       /* non-finite or non-positive P, T or z (reference throws) */
 #define NZ_FLASH_EOS_ERROR 3       /* no admissible cubic root etc. (reference throws) */
 #define NZ_FLASH_NOT_PORTED 4      /* reached a fail-only recovery this build does not carry */
+#define NZ_FLASH_UNFINISHED 5      /* a device self-check of the staged batch stopped before this
+                                      point was done (see nz_flash_check); no reference counterpart */
 
 /* ---- fluid description --------------------------------------------------
  * Mirrors CompositionalMixture + CubicEquationOfState configuration
@@ -183,7 +186,8 @@ typedef struct nz_flash_out {
 
 #define NZ_PRECISION_FP64 0         /* plain FP64 form: one thread runs one point's whole flash */
 #define NZ_PRECISION_MIXED 1        /* staged; leading SSI steps of the TPD trials with FP32 mixing and
-                                       ln phi (FP64 root), every trial finished in FP64 */
+                                       ln phi (FP64 root), every trial finished in FP64, and a final FP64
+                                       ln-fugacity Newton polish of the multiphase answers to 1e-11 */
 #define NZ_PRECISION_FP64_STAGED 2  /* staged, every TPD trial in FP64 exactly as the plain form */
 
 int nz_flash_batch(nz_ctx* ctx, int64_t n, const double* pressure,
@@ -200,6 +204,20 @@ int nz_flash_batch_host(nz_ctx* ctx, int64_t n, const double* pressure,
 /* Number of single-phase EOS evaluations (mixing+root+ln phi) the last
  * nz_flash_batch on this context executed; read after a stream sync. */
 int nz_flash_eos_eval_count(nz_ctx* ctx, uint64_t* count);
+
+/* Self-checks of the last staged batch on this context (no counterpart in the
+ * reference, which has no device queues).  The staged kernels bound every
+ * queue they fill and cap every lane-refill loop; a tripped check sets a
+ * code here (0 = none), the kernels after it leave the unfinished points
+ * alone, and those points keep status NZ_FLASH_UNFINISHED.  Read after the
+ * batch's stream has been synchronised.  nz_flash_batch_host makes this
+ * check itself and returns NZ_ERR_SELFCHECK when a code is set. */
+int nz_flash_check(nz_ctx* ctx, int32_t* bound_code, int32_t* guard_code);
+
+/* Iterations a lane-refill loop of the staged kernels may run before it gives
+ * up (default 2^26, far above any solve); >= 1.  Lowering it is how a caller
+ * (or a test) makes the spin guard run out without faulting the GPU. */
+int nz_ctx_set_spin_limit(nz_ctx* ctx, int64_t limit);
 
 /* ---- P-T-z flash without allocation ------------------------------------------
  * No counterpart in the reference (it has no GPU code): an extra entry point

@@ -14,13 +14,15 @@ NZ_RECOVERABLE = 1
 NZ_ERR_ARGUMENT = -1
 NZ_ERR_CUDA = -2
 NZ_ERR_UNSUPPORTED = -3
+NZ_ERR_ALLOC = -4
+NZ_ERR_SELFCHECK = -5
 
 EOS_PR, EOS_SW, EOS_CPA = 0, 1, 2
 CPA_SRK, CPA_PR = 0, 1
 CPA_RADIAL_SIMPLIFIED, CPA_RADIAL_CARNAHAN_STARLING = 0, 1
 SW_BIP_KIJ, SW_BIP_CONSTANT, SW_BIP_CO2, SW_BIP_HYDROCARBON, SW_BIP_CO2_CHABAB = range(5)
 
-FLASH_CONVERGED, FLASH_FAILED, FLASH_BAD_INPUT, FLASH_EOS_ERROR, FLASH_NOT_PORTED = range(5)
+FLASH_CONVERGED, FLASH_FAILED, FLASH_BAD_INPUT, FLASH_EOS_ERROR, FLASH_NOT_PORTED, FLASH_UNFINISHED = range(6)
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1

@@ -11,6 +11,11 @@ namespace nz
 {
 
 constexpr int kFlashBlock = 128;
+// nz_ctx::evalCounter block: the EOS evaluation count (8 bytes), then the
+// last batch's two self-check words (queue bound, spin guard).
+constexpr size_t kCounterBlockBytes = 16;
+// Default iteration cap of the lane-refill loops (FluidDev::spinLimit).
+constexpr long long kDefaultSpinLimit = 1LL << 26;
 constexpr int kTrialBlock = 128;
 constexpr int kTrialBlocksPerSm = 8;
 
@@ -29,6 +34,7 @@ struct nz_ctx
     nz_flash_options options{};
     nz::FluidDev fluid{};
     unsigned long long *evalCounter{nullptr};   // EOS evaluations of the last flash batch
+    int *checkWords{nullptr};                   // its self-check words (inside the evalCounter block)
     cudaStream_t ownStream{nullptr};
     int smCount{148};
     void *scratch{nullptr};                     // staged-flash work space (grow only)
@@ -59,6 +65,12 @@ size_t stagedScratchBytesFor(int nc, int64_t n, const FluidDev &F);
 int64_t stagedMaxPointsFor(int nc, size_t capacity, const FluidDev &F);
 template <int NC>
 size_t stagedScratchBytesNc(int64_t n, const FluidDev &F);
+// The staged launch sequence (defined in staged_inst.cu) for callers in other
+// translation units; the scratch block holds stagedScratchBytesNc<NC>(n) bytes.
+template <int NC>
+int stagedLaunchExt(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
+                    const double *z, const double *sal, const nz_flash_out &out,
+                    unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed);
 }
 
 // Runtime nc -> compile-time NC dispatch over the instantiated component counts.

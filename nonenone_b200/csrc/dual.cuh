@@ -114,6 +114,233 @@ NZ_BOTH Dual cos(const Dual &x) { return Dual(::cos(x.v), (-::sin(x.v)) * x.d); 
 NZ_BOTH Dual abs(const Dual &x) { return (x.v >= 0.0) ? x : -x; }
 NZ_BOTH double abs(double x) { return ::fabs(x); }
 
+// K-direction dual number: the value and the derivatives along K of the
+// cell's primary unknowns, so one lane carries K columns of a Jacobian block
+// and a cell needs ceil(B / K) lanes instead of B -- the value path, which
+// each lane recomputes, runs B / K times fewer per cell.  Every derivative
+// component follows exactly the one-direction rule of Dual above.
+template <int K>
+struct DualN
+{
+    double v;
+    double d[K];
+
+    NZ_BOTH DualN() : v(0.0)
+    {
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            d[j] = 0.0;
+    }
+    NZ_BOTH DualN(double value) : v(value)
+    {
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            d[j] = 0.0;
+    }
+};
+
+template <int K>
+NZ_BOTH double val(const DualN<K> &x) { return x.v; }
+template <int K>
+NZ_BOTH void clearDer(DualN<K> &x)
+{
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        x.d[j] = 0.0;
+}
+
+// A primary unknown of index `idx` for a lane whose directions start at
+// `k` (k >= 0; a Dual lane has the one direction k): Seed<S>::at(value, idx, k).
+template <class S>
+struct Seed;
+template <>
+struct Seed<double>
+{
+    NZ_BOTH static double at(double value, int, int) { return value; }
+};
+template <>
+struct Seed<Dual>
+{
+    NZ_BOTH static Dual at(double value, int idx, int k) { return idx == k ? Dual(value, 1.0) : Dual(value); }
+};
+template <int K>
+struct Seed<DualN<K>>
+{
+    NZ_BOTH static DualN<K> at(double value, int idx, int k)
+    {
+        DualN<K> r(value);
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            r.d[j] = idx == k + j ? 1.0 : 0.0;
+        return r;
+    }
+};
+
+#define NZ_DUALN_BINARY(OP, VALUE, DERIV)                                                \
+    template <int K>                                                                     \
+    NZ_BOTH DualN<K> operator OP(const DualN<K> &a, const DualN<K> &b)                   \
+    {                                                                                    \
+        DualN<K> r;                                                                      \
+        r.v = VALUE;                                                                     \
+        _Pragma("unroll") for (int j = 0; j < K; ++j) r.d[j] = DERIV;                    \
+        return r;                                                                        \
+    }
+NZ_DUALN_BINARY(+, a.v + b.v, a.d[j] + b.d[j])
+NZ_DUALN_BINARY(-, a.v - b.v, a.d[j] - b.d[j])
+NZ_DUALN_BINARY(*, a.v * b.v, a.d[j] * b.v + b.d[j] * a.v)
+NZ_DUALN_BINARY(/, a.v / b.v, (b.v * a.d[j] - a.v * b.d[j]) / (b.v * b.v))
+#undef NZ_DUALN_BINARY
+
+template <int K>
+NZ_BOTH DualN<K> operator-(const DualN<K> &a)
+{
+    DualN<K> r;
+    r.v = -a.v;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = -a.d[j];
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator+(const DualN<K> &a, double b)
+{
+    DualN<K> r = a;
+    r.v = a.v + b;
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator+(double a, const DualN<K> &b)
+{
+    DualN<K> r = b;
+    r.v = b.v + a;
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator-(const DualN<K> &a, double b)
+{
+    DualN<K> r = a;
+    r.v = a.v - b;
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator-(double a, const DualN<K> &b)
+{
+    DualN<K> r;
+    r.v = -b.v + a;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = -b.d[j];
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator*(const DualN<K> &a, double b)
+{
+    DualN<K> r;
+    r.v = a.v * b;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = a.d[j] * b;
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator*(double a, const DualN<K> &b)
+{
+    DualN<K> r;
+    r.v = b.v * a;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = b.d[j] * a;
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator/(const DualN<K> &a, double b)
+{
+    const double q = 1.0 / b;
+    DualN<K> r;
+    r.v = a.v * q;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = a.d[j] * q;
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> operator/(double a, const DualN<K> &b)
+{
+    DualN<K> r;
+    r.v = a / b.v;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = (b.v * 0.0 - a * b.d[j]) / (b.v * b.v);
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> &operator+=(DualN<K> &a, const DualN<K> &b)
+{
+    a.v += b.v;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        a.d[j] += b.d[j];
+    return a;
+}
+template <int K>
+NZ_BOTH DualN<K> &operator+=(DualN<K> &a, double b)
+{
+    a.v += b;
+    return a;
+}
+template <int K>
+NZ_BOTH DualN<K> &operator-=(DualN<K> &a, const DualN<K> &b)
+{
+    a.v -= b.v;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        a.d[j] -= b.d[j];
+    return a;
+}
+// f(x) with f' given: the same scalar factor as Dual's rules, times each direction
+template <int K>
+NZ_BOTH DualN<K> chainN(double value, double factor, const DualN<K> &x)
+{
+    DualN<K> r;
+    r.v = value;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = factor * x.d[j];
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> sqrt(const DualN<K> &x)
+{
+    const double s = ::sqrt(x.v);
+    return chainN(s, 0.5 / s, x);
+}
+template <int K>
+NZ_BOTH DualN<K> exp(const DualN<K> &x)
+{
+    const double e = ::exp(x.v);
+    DualN<K> r;
+    r.v = e;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        r.d[j] = e * x.d[j];
+    return r;
+}
+template <int K>
+NZ_BOTH DualN<K> log(const DualN<K> &x) { return chainN(::log(x.v), 1.0 / x.v, x); }
+template <int K>
+NZ_BOTH DualN<K> pow(const DualN<K> &x, double p)
+{
+    if (p == 0.0)
+        return DualN<K>(::pow(x.v, p));
+    return chainN(::pow(x.v, p), p * ::pow(x.v, p - 1.0), x);
+}
+template <int K>
+NZ_BOTH DualN<K> acos(const DualN<K> &x) { return chainN(::acos(x.v), -1.0 / ::sqrt(1.0 - x.v * x.v), x); }
+template <int K>
+NZ_BOTH DualN<K> cos(const DualN<K> &x) { return chainN(::cos(x.v), -::sin(x.v), x); }
+template <int K>
+NZ_BOTH DualN<K> abs(const DualN<K> &x) { return (x.v >= 0.0) ? x : -x; }
+
 // Value-only scalar with the AD type's rounding.  The reference evaluates cell
 // properties and local residuals in its AD type even when only values are
 // used (the residual's cell cache), so value kernels use this type to round
@@ -131,6 +358,11 @@ NZ_BOTH double der(const Val &) { return 0.0; }
 NZ_BOTH void clearDer(Val &) {}
 template <>
 NZ_BOTH Val makeSeeded<Val>(double value) { return Val(value); }
+template <>
+struct Seed<Val>
+{
+    NZ_BOTH static Val at(double value, int, int) { return Val(value); }
+};
 
 NZ_BOTH Val operator-(const Val &a) { return Val(-a.v); }
 NZ_BOTH Val operator+(const Val &a, const Val &b) { return Val(a.v + b.v); }

@@ -149,6 +149,10 @@ struct FluidDev
     double swValue[kMaxNc];
     FlashOpts opt;
     CpaDev cpa;
+    // Iterations a lane-refill loop of the staged kernels may run before it
+    // gives up and sets the batch's guard word (a self-check, not a
+    // convergence limit: the solves end far earlier).
+    long long spinLimit;
 };
 
 template <int NC>

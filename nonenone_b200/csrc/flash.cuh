@@ -3578,6 +3578,206 @@ struct Solver
         return CONT_SUCCESS;
     }
 
+    // ---------------------------------------------------------- polish --
+    // Final ln-fugacity Newton polish of a converged multiphase result (no
+    // reference counterpart: the reference stops at its 1e-9 ln K tolerance,
+    // which leaves ln-fugacity differences up to ~1e-9).  Newton on ln K with
+    // the flash's own residual (evalTwo / evalThree: Rachford-Rice inside) and
+    // a forward-difference Jacobian, until the largest residual is below
+    // `target` or `maxSteps` steps are done.  `r` is replaced only by a state
+    // with the same phases and a smaller residual; an error inside leaves `r`
+    // and `err` as they were.  Returns true when `r` was replaced.
+    NZ_HDN bool polish(double P, double T, const double *z, Result<NC> &r, double target, int maxSteps)
+    {
+        if (!r.converged)
+            return false;
+        const int errBefore = err;
+        err = ERR_NONE;
+        bool replaced = false;
+        const int count = popcount3(r.presence);
+        if (count == 2)
+            replaced = polishTwo(P, T, z, r, target, maxSteps);
+        else if (count == 3)
+            replaced = polishThree(P, T, z, r, target, maxSteps);
+        err = errBefore;
+        return replaced;
+    }
+
+    NZ_HDN bool polishTwo(double P, double T, const double *z, Result<NC> &r, double target, int maxSteps)
+    {
+        int first, second;
+        activePair(r.presence, first, second);
+        double logK[NC];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+            logK[i] = log(smax(r.x[second][i], O().floor) / smax(r.x[first][i], O().floor));
+        TwoPhaseLogKState<NC> base, probe;
+        evalTwo(P, T, z, first, second, logK, r.beta[second], base);
+        if (!base.valid || err)
+            return false;
+        const double start = base.norm;
+        bool moved = false;
+#pragma unroll 1
+        for (int step = 0; step < maxSteps && base.norm > target; ++step)
+        {
+            double J[NC][NC];
+            bool ok = true;
+#pragma unroll 1
+            for (int col = 0; col < NC && ok; ++col)
+            {
+                double pert[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    pert[i] = logK[i];
+                const double h = O().fdStep * smax(1.0, fabs(logK[col]));
+                pert[col] += h;
+                evalTwo(P, T, z, first, second, pert, base.result.beta[second], probe);
+                ok = probe.valid && !err;
+                if (ok)
+#pragma unroll
+                    for (int row = 0; row < NC; ++row)
+                        J[row][col] = (probe.residual[row] - base.residual[row]) / h;
+            }
+            double rhs[NC], delta[NC];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                rhs[i] = -base.residual[i];
+            if (!ok || !solveDense<NC>(J, rhs, delta))
+                break;
+            bool accepted = false;
+            double damping = 1.0;
+#pragma unroll 1
+            for (int ls = 0; ls < 8 && !accepted; ++ls, damping *= 0.5)
+            {
+                double trial[NC];
+#pragma unroll
+                for (int i = 0; i < NC; ++i)
+                    trial[i] = logK[i] + damping * delta[i];
+                evalTwo(P, T, z, first, second, trial, base.result.beta[second], probe);
+                if (probe.valid && !err && probe.norm < base.norm)
+                {
+#pragma unroll
+                    for (int i = 0; i < NC; ++i)
+                        logK[i] = trial[i];
+                    base = probe;
+                    accepted = moved = true;
+                }
+            }
+            if (!accepted)
+                break;
+        }
+        if (!moved || !(base.norm < start))
+            return false;
+        Result<NC> q = r;
+        q.beta[0] = q.beta[1] = q.beta[2] = 0.0;
+        q.beta[first] = base.result.beta[first];
+        q.beta[second] = base.result.beta[second];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            q.x[first][i] = base.result.x[first][i];
+            q.x[second][i] = base.result.x[second][i];
+        }
+        q.Z[first] = base.result.Z[first];
+        q.Z[second] = base.result.Z[second];
+        if (presenceFromFractions(q.beta) != r.presence)
+            return false;
+        deriveReferenceK(q);
+        updateSaturations(P, T, q);
+        if (err)
+            return false;
+        r = q;
+        return true;
+    }
+
+    NZ_HDN bool polishThree(double P, double T, const double *z, Result<NC> &r, double target, int maxSteps)
+    {
+        constexpr int M = 2 * NC;
+        double logK[M];
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+        {
+            const double xo = smax(r.x[0][i], O().floor);
+            logK[i] = log(smax(r.x[1][i], O().floor) / xo);
+            logK[NC + i] = log(smax(r.x[2][i], O().floor) / xo);
+        }
+        ThreePhaseLogKState<NC> base, probe;
+        evalThree(P, T, z, logK, r.beta[1], r.beta[2], base);
+        if (!base.valid || err)
+            return false;
+        const double start = base.norm;
+        bool moved = false;
+#pragma unroll 1
+        for (int step = 0; step < maxSteps && base.norm > target; ++step)
+        {
+            double J[M][M];
+            bool ok = true;
+#pragma unroll 1
+            for (int col = 0; col < M && ok; ++col)
+            {
+                double pert[M];
+#pragma unroll
+                for (int i = 0; i < M; ++i)
+                    pert[i] = logK[i];
+                const double h = O().fdStep * smax(1.0, fabs(logK[col]));
+                pert[col] += h;
+                evalThree(P, T, z, pert, base.result.beta[1], base.result.beta[2], probe);
+                ok = probe.valid && !err;
+                if (ok)
+#pragma unroll
+                    for (int row = 0; row < M; ++row)
+                        J[row][col] = (probe.residual[row] - base.residual[row]) / h;
+            }
+            double rhs[M], delta[M];
+#pragma unroll
+            for (int i = 0; i < M; ++i)
+                rhs[i] = -base.residual[i];
+            if (!ok || !solveDense<M>(J, rhs, delta))
+                break;
+            bool accepted = false;
+            double damping = 1.0;
+#pragma unroll 1
+            for (int ls = 0; ls < 8 && !accepted; ++ls, damping *= 0.5)
+            {
+                double trial[M];
+#pragma unroll
+                for (int i = 0; i < M; ++i)
+                    trial[i] = logK[i] + damping * delta[i];
+                evalThree(P, T, z, trial, base.result.beta[1], base.result.beta[2], probe);
+                if (probe.valid && !err && probe.norm < base.norm)
+                {
+#pragma unroll
+                    for (int i = 0; i < M; ++i)
+                        logK[i] = trial[i];
+                    base = probe;
+                    accepted = moved = true;
+                }
+            }
+            if (!accepted)
+                break;
+        }
+        if (!moved || !(base.norm < start))
+            return false;
+        Result<NC> q = r;
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+        {
+            q.beta[p] = base.result.beta[p];
+            q.Z[p] = base.result.Z[p];
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                q.x[p][i] = base.result.x[p][i];
+        }
+        if (presenceFromFractions(q.beta) != r.presence)
+            return false;
+        deriveReferenceK(q);
+        updateSaturations(P, T, q);
+        if (err)
+            return false;
+        r = q;
+        return true;
+    }
+
     // pressureContinuationFallback_ (restricted.inc:554-627): anchors in order.
     NZ_HDN void pressureContinuation(double P, double T, const double *z, Result<NC> &out)
     {

@@ -1,4 +1,6 @@
-// nat_inst.cu -- Natural kernels of one component count (NZ_INST_NC).
+// natstate_inst.cu -- the Natural phase-state kernels (per-cell and staged
+// update, P-T-z initialisation) of one component count, and the dispatch of
+// every Natural operation (the assembly kernels live in natasm_inst.cu).
 #include "natural_host.cuh"
 #include "natural_kernels.cuh"
 #include "natural_staged.cuh"
@@ -10,10 +12,12 @@
 namespace nz
 {
 template <int NC>
+int natLaunchAssembly(int op, const NatLaunch &a, cudaStream_t st);
+
+template <int NC>
 int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
 {
     const int64_t n = a.g.ncell;
-    const unsigned grid = unsigned((n + kNatBlock - 1) / kNatBlock);
     // Phase-state solves: a warp per cell while the cells cannot fill the GPU
     // with threads, a thread per cell beyond that.
     int device = 0, smCount = 148;
@@ -24,23 +28,10 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
     switch (op)
     {
     case NAT_CACHE:
-        natCacheKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.flag);
-        break;
     case NAT_RESIDUAL:
-        natResidualKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.residual, a.flag);
-        break;
     case NAT_JACOBIAN:
-    {
-        constexpr int perWarp = 32 / Layout<NC>::B;
-        const int64_t warps = (n + perWarp - 1) / perWarp;
-        const unsigned jgrid = unsigned((warps * 32 + kNatBlock - 1) / kNatBlock);
-        natJacobianKernel<NC><<<jgrid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.values, a.residual,
-                                                          a.flag);
-        break;
-    }
     case NAT_HISTORY:
-        natHistoryKernel<NC><<<grid, kNatBlock, 0, st>>>(a.F, a.K, a.g, a.primary, a.ps, a.prevAcc, a.flag);
-        break;
+        return natLaunchAssembly<NC>(op, a, st);
     case NAT_UPDATE_PREPARE:
         return natStagedStability<NC>(a.F, a.K, n, a.primary, a.ps, a.stagedScratch, smCount, st);
     case NAT_UPDATE_REFLASH:

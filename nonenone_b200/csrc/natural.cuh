@@ -117,15 +117,14 @@ NZ_HD void decodeCell(const double *primary, double flag, int k, CellStateT<NC, 
 {
     using L = Layout<NC>;
     st.presence = decodePresence(flag);
-    st.p = S(primary[0]);
-    if (k == 0) st.p = makeSeeded<S>(primary[0]);
+    st.p = Seed<S>::at(primary[0], 0, k);
     for (int ph = 0; ph < 3; ++ph)
     {
         S dependent = S(1.0);
         for (int i = 0; i < NC - 1; ++i)
         {
             const int idx = L::comp(ph, i);
-            st.x[ph][i] = idx == k ? makeSeeded<S>(primary[idx]) : S(primary[idx]);
+            st.x[ph][i] = Seed<S>::at(primary[idx], idx, k);
             dependent = dependent - st.x[ph][i];
         }
         const double dv = val(dependent);
@@ -135,7 +134,7 @@ NZ_HD void decodeCell(const double *primary, double flag, int k, CellStateT<NC, 
     }
     const int sIdx[3] = {L::So, L::Sg, L::Sw};
     for (int ph = 0; ph < 3; ++ph)
-        st.sat[ph] = sIdx[ph] == k ? makeSeeded<S>(primary[sIdx[ph]]) : S(primary[sIdx[ph]]);
+        st.sat[ph] = Seed<S>::at(primary[sIdx[ph]], sIdx[ph], k);
 }
 
 // ---- EOS in S (cubic_eos.hpp) -------------------------------------------

@@ -368,6 +368,149 @@ __global__ void __launch_bounds__(kNatBlock) natJacobianKernel(const __grid_cons
         atomicOr(flag, 1);
 }
 
+// Lane layout of natJacobianKernelN with KD directions per lane.
+template <int NC, int KD>
+struct JacobianShape
+{
+    static constexpr int B = Layout<NC>::B;
+    static constexpr int K = KD;                     // directions per lane
+    static constexpr int G = (B + K - 1) / K;        // lanes per cell
+    static constexpr int perWarp = 32 / G;           // cells per warp
+    static constexpr int warps = kNatBlock / 32;
+    static constexpr size_t smemBytes = size_t(warps) * perWarp * B * B * sizeof(double);
+};
+
+// The BAIJ Jacobian with K directions per lane (DualN<K>): G = ceil(B / K)
+// lanes per cell, so the value part of a cell's properties -- transcendental
+// heavy, and recomputed by every lane -- runs G times per cell instead of B.
+// Every block of the warp's cells is assembled in shared memory and stored to
+// its BAIJ slot as one contiguous B*B*8-byte range by the whole warp (whole
+// 32-byte sectors), the reciprocal blocks face by face in connection order and
+// the self block last, with the face rows added into it in the same order as
+// the one-direction kernel (jacobian.inc:120-237).
+template <int NC, int KDIR>
+__global__ void __launch_bounds__(kNatBlock) natJacobianKernelN(const __grid_constant__ FluidDev F,
+                                                                const __grid_constant__ NatConst K, NatGeom g,
+                                                                const double *primary, const double *ps,
+                                                                double *values, double *residual, int *flag)
+{
+    using L = Layout<NC>;
+    using J = JacobianShape<NC, KDIR>;
+    constexpr int B = L::B;
+    constexpr int KD = J::K;
+    constexpr int G = J::G;
+    constexpr int perWarp = J::perWarp;
+    constexpr int BB = B * B;
+    using S = DualN<KD>;
+    extern __shared__ double natTile[];
+    const int lane = threadIdx.x & 31;
+    const int warpInBlock = threadIdx.x >> 5;
+    double *tile = natTile + size_t(warpInBlock) * perWarp * BB;
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int group = lane / G;
+    const int sub = lane - group * G;
+    const int k0 = sub * KD;
+    const int64_t c = warp * perWarp + group;
+    const bool mine = group < perWarp && c < g.ncell;
+
+    CellStateT<NC, S> st;
+    CellPropsT<NC, S> pr;
+    S res[B];
+    bool ok = false;
+    if (mine)
+    {
+        decodeCell<NC, S>(primary + c * B, ps[c * L::NPS + L::psFlag], k0, st);
+        ok = st.presence != 0 && cellProperties<NC, S>(F, K, st, g.porosity[c], pr);
+        if (ok)
+            localResidual<NC, S>(K, st, pr, g.prevAcc + c * NC, g.volume[c], res);
+        else if (sub == 0)
+            atomicOr(flag, 1);
+    }
+    const bool wantResidual = ok && residual && sub == 0;
+    FaceSide<NC> inVal;
+    if (wantResidual)
+    {
+        inVal.p = st.p.v;
+        for (int ph = 0; ph < 3; ++ph)
+        {
+            inVal.density[ph] = pr.density[ph].v;
+            inVal.saturation[ph] = pr.saturation[ph].v;
+            inVal.mobility[ph] = pr.mobility[ph].v;
+            for (int i = 0; i < NC; ++i)
+                inVal.w[ph][i] = pr.w[ph][i].v;
+        }
+    }
+    double outward[NC];
+    for (int i = 0; i < NC; ++i)
+        outward[i] = 0.0;
+    const int64_t first = ok ? g.offset[c] : 0;
+    const int nfaces = ok ? int(g.offset[c + 1] - first) : 0;
+    int maxFaces = nfaces;
+    for (int off = 16; off > 0; off >>= 1)
+        maxFaces = max(maxFaces, __shfl_xor_sync(0xffffffffu, maxFaces, off));
+    double *myTile = tile + (group < perWarp ? group : 0) * BB;
+
+    // store the tiles of the warp's cells that have a block in this pass
+    auto flush = [&](bool has, int64_t slot) {
+        __syncwarp();
+        for (int e = lane; e < perWarp * BB; e += 32)
+        {
+            const int q = e / BB;
+            const int o = e - q * BB;
+            const int owner = q * G;
+            const int qHas = __shfl_sync(0xffffffffu, int(has), owner);
+            const long long qSlot = __shfl_sync(0xffffffffu, (long long)slot, owner);
+            if (qHas)
+                values[qSlot * BB + o] = tile[e];
+        }
+        __syncwarp();
+    };
+
+    for (int f = 0; f < maxFaces; ++f)
+    {
+        const bool has = f < nfaces;
+        int64_t slot = 0;
+        if (has)
+        {
+            const int64_t j = first + f;
+            const int64_t nb = g.neighbor[j];
+            FaceSide<NC> ex;
+            loadSide<NC>(g.cache, g.ncell, nb, ex);
+            S flux[NC];
+            faceFlux<NC, S>(st, pr, ex, g.trans[j], g.gravity[j], g.volume[c], g.volume[nb], c, nb, flux);
+            for (int i = 0; i < NC; ++i)
+                for (int jj = 0; jj < KD; ++jj)
+                    res[L::mass + i].d[jj] += flux[i].d[jj];
+            for (int r = 0; r < B; ++r)
+                for (int jj = 0; jj < KD; ++jj)
+                    if (k0 + jj < B)
+                        myTile[r * B + k0 + jj] = r < NC ? -flux[r].d[jj] : 0.0;
+            slot = g.connSlot[j];
+            if (wantResidual)
+            {
+                double fv[NC];
+                faceFluxValue<NC>(inVal, ex, g.trans[j], g.gravity[j], g.volume[c], g.volume[nb], c, nb, fv);
+                for (int i = 0; i < NC; ++i)
+                    outward[i] += fv[i];
+            }
+        }
+        flush(has, slot);
+    }
+    if (ok)
+        for (int r = 0; r < B; ++r)
+            for (int jj = 0; jj < KD; ++jj)
+                if (k0 + jj < B)
+                    myTile[r * B + k0 + jj] = res[r].d[jj];
+    flush(ok, ok ? g.selfSlot[c] : 0);
+    if (wantResidual)
+    {
+        for (int i = 0; i < NC; ++i)
+            res[L::mass + i].v += outward[i];
+        for (int r = 0; r < B; ++r)
+            residual[c * B + r] = res[r].v;
+    }
+}
+
 template <int NC>
 __global__ void __launch_bounds__(kNatBlock) natHistoryKernel(const __grid_constant__ FluidDev F,
                                                               const __grid_constant__ NatConst K, NatGeom g,

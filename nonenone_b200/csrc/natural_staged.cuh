@@ -378,7 +378,7 @@ int natReflash(const FluidDev &F, int64_t ncell, void *scratch, void *flashScrat
     out.k_water_oil = out.k_gas_oil + NC * size_t(n);
     const unsigned grid = unsigned((n + 255) / 256);
     natGatherKernel<NC><<<grid, 256, 0, st>>>(n, w, P, T, z);
-    int rc = stagedLaunch<NC>(F, flashScratch, n, P, T, z, nullptr, out, evals, smCount, st);
+    int rc = stagedLaunchExt<NC>(F, flashScratch, n, P, T, z, nullptr, out, evals, smCount, st, false);
     if (rc != 0)
         return rc;
     natScatterKernel<NC><<<grid, 256, 0, st>>>(n, w, P, T, z, out);

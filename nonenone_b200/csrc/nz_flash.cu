@@ -114,6 +114,7 @@ FluidDev makeFluidDev(const nz_fluid_desc &d, const nz_flash_options &o)
     f.opt.floor = o.composition_floor;
     f.opt.logKLimit = o.log_k_step_limit;
     f.opt.fdStep = o.numerical_jacobian_step;
+    f.spinLimit = kDefaultSpinLimit;
     return f;
 }
 
@@ -198,13 +199,15 @@ int nz_ctx_create(const nz_fluid_desc *fluid, const nz_flash_options *options, i
     c->options = opts;
     c->fluid = makeFluidDev(*fluid, opts);
     cudaDeviceGetAttribute(&c->smCount, cudaDevAttrMultiProcessorCount, device);
-    e = cudaMalloc(&c->evalCounter, sizeof(unsigned long long));
+    // evaluation counter, then the two self-check words of the last batch
+    e = cudaMalloc(&c->evalCounter, kCounterBlockBytes);
     if (e != cudaSuccess)
     {
         delete c;
         return cudaFail(e, "cudaMalloc(eval counter)");
     }
-    cudaMemset(c->evalCounter, 0, sizeof(unsigned long long));
+    c->checkWords = reinterpret_cast<int *>(c->evalCounter + 1);
+    cudaMemset(c->evalCounter, 0, kCounterBlockBytes);
     *out = c;
     return NZ_OK;
 }
@@ -258,7 +261,7 @@ int nz_flash_batch(nz_ctx *ctx, int64_t n, const double *P, const double *T, con
         precision != NZ_PRECISION_FP64_STAGED)
         return setError(NZ_ERR_ARGUMENT, "nz_flash_batch: unknown precision %d", precision);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(ctx->evalCounter, 0, sizeof(unsigned long long), st);
+    cudaError_t e = cudaMemsetAsync(ctx->evalCounter, 0, kCounterBlockBytes, st);
     if (e != cudaSuccess)
         return cudaFail(e, "nz_flash_batch counter reset");
     if (n == 0)
@@ -353,7 +356,40 @@ int nz_flash_batch_host(nz_ctx *ctx, int64_t n, const double *P, const double *T
     e = cudaStreamSynchronize(st);
     if (rc == NZ_OK && e != cudaSuccess)
         rc = cudaFail(e, "nz_flash_batch_host sync");
+    if (rc == NZ_OK && precision != NZ_PRECISION_FP64)
+    {
+        int32_t bound = 0, guard = 0;
+        rc = nz_flash_check(ctx, &bound, &guard);
+        if (rc == NZ_OK && (bound || guard))
+            rc = setError(NZ_ERR_SELFCHECK,
+                          "nz_flash_batch_host: a device self-check stopped the batch (queue bound %d, spin guard %d); "
+                          "points it left have status NZ_FLASH_UNFINISHED",
+                          bound, guard);
+    }
     return rc;
+}
+
+int nz_flash_check(nz_ctx *ctx, int32_t *bound_code, int32_t *guard_code)
+{
+    if (!ctx)
+        return setError(NZ_ERR_ARGUMENT, "nz_flash_check: null context");
+    int words[2] = {0, 0};
+    cudaError_t e = cudaMemcpy(words, ctx->checkWords, sizeof(words), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cudaFail(e, "nz_flash_check");
+    if (bound_code)
+        *bound_code = words[0];
+    if (guard_code)
+        *guard_code = words[1];
+    return NZ_OK;
+}
+
+int nz_ctx_set_spin_limit(nz_ctx *ctx, int64_t limit)
+{
+    if (!ctx || limit < 1)
+        return setError(NZ_ERR_ARGUMENT, "nz_ctx_set_spin_limit: need a context and a limit >= 1");
+    ctx->fluid.spinLimit = limit;
+    return NZ_OK;
 }
 
 } // extern "C"

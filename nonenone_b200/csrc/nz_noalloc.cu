@@ -66,7 +66,7 @@ extern "C" int nz_flash_batch_noalloc(nz_ctx *ctx, int64_t n, const double *P, c
     if (rc != NZ_OK)
         return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(ctx->evalCounter, 0, sizeof(unsigned long long), st);
+    cudaError_t e = cudaMemsetAsync(ctx->evalCounter, 0, kCounterBlockBytes, st);
     if (e != cudaSuccess)
         return cudaFail(e, "nz_flash_batch_noalloc counter reset");
     if (n == 0)

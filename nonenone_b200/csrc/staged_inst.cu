@@ -1,7 +1,5 @@
-// nz_inst.cu -- explicit instantiation of the per-component-count kernels.
-// Compiled once per NZ_INST_NC value (3, 4, 5, 6, 8) so the heavy device code
-// of each component count builds in its own translation unit.
-#include "flash_kernels.cuh"
+// staged_inst.cu -- the staged batched flash of one component count
+// (NZ_INST_NC): its launch sequence and work-space sizes.
 #include "staged_kernels.cuh"
 
 #ifndef NZ_INST_NC
@@ -10,13 +8,6 @@
 
 namespace nz
 {
-template int launchFlash<NZ_INST_NC>(nz_ctx *, int64_t, const double *, const double *, const double *,
-                                     const double *, const nz_flash_out &, cudaStream_t);
-template int launchEos<NZ_INST_NC>(nz_ctx *, int64_t, const double *, const double *, const double *,
-                                   const int8_t *, const double *, double *, double *, cudaStream_t);
-template int launchStability<NZ_INST_NC>(nz_ctx *, int64_t, const double *, const double *, const double *,
-                                         const double *, const uint8_t *, const double *, uint8_t *,
-                                         uint8_t *, uint8_t *, double *, double *, cudaStream_t);
 template <int NC>
 int launchStaged(nz_ctx *ctx, int64_t n, const double *P, const double *T, const double *z,
                  const double *sal, const nz_flash_out &out, bool mixed, cudaStream_t st)
@@ -26,7 +17,7 @@ int launchStaged(nz_ctx *ctx, int64_t n, const double *P, const double *T, const
     if (rc != 0)
         return rc;
     return stagedLaunch<NC>(ctx->fluid, ctx->scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st,
-                            mixed);
+                            mixed, ctx->checkWords);
 }
 template <int NC>
 int launchStagedInto(nz_ctx *ctx, void *scratch, size_t capacity, int64_t n, const double *P, const double *T,
@@ -35,13 +26,23 @@ int launchStagedInto(nz_ctx *ctx, void *scratch, size_t capacity, int64_t n, con
     if (stagedScratchBytes<NC>(n, ctx->fluid) > capacity)
         return setError(NZ_ERR_ARGUMENT, "staged flash: work space too small");
     return stagedLaunch<NC>(ctx->fluid, scratch, n, P, T, z, sal, out, ctx->evalCounter, ctx->smCount, st,
-                            mixed);
+                            mixed, ctx->checkWords);
 }
 template <int NC>
 size_t stagedScratchBytesNc(int64_t n, const FluidDev &F)
 {
     return stagedScratchBytes<NC>(n, F);
 }
+template <int NC>
+int stagedLaunchExt(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
+                    const double *z, const double *sal, const nz_flash_out &out,
+                    unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed)
+{
+    return stagedLaunch<NC>(F, scratch, n, P, T, z, sal, out, evalCounter, smCount, st, mixed);
+}
+template int stagedLaunchExt<NZ_INST_NC>(const FluidDev &, void *, int64_t, const double *, const double *,
+                                         const double *, const double *, const nz_flash_out &,
+                                         unsigned long long *, int, cudaStream_t, bool);
 template int launchStagedInto<NZ_INST_NC>(nz_ctx *, void *, size_t, int64_t, const double *, const double *,
                                           const double *, const double *, const nz_flash_out &, bool,
                                           cudaStream_t);

@@ -116,6 +116,28 @@ inline int64_t contCapacity(int64_t n)
     return n / 32 < 64 ? 64 : n / 32;
 }
 
+// A queue bound or a spin guard has tripped in this batch: the kernels that
+// follow leave the unfinished points alone (their status stays
+// NZ_FLASH_UNFINISHED) instead of building on incomplete queues.  The test is
+// warp-uniform (read at kernel entry with every lane of the warp active), so a
+// warp leaves as a whole and no lane waits at a warp-wide operation.
+__device__ __forceinline__ bool stagedTripped(const StagedArgs &a)
+{
+    const bool tripped = a.counters[kCounterBound] != 0 || a.counters[kCounterGuard] != 0;
+    return __any_sync(0xffffffffu, tripped);
+}
+
+// After the last kernel of a batch: copy its queue-bound and spin-guard codes
+// to `sink` ([0] bound, [1] guard; the context's check words), if given.
+static __global__ void stagedCheckKernel(const int *counters, int *sink)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0 && sink)
+    {
+        sink[0] = counters[kCounterBound];
+        sink[1] = counters[kCounterGuard];
+    }
+}
+
 // Dispatch a point after its driver returned.
 template <int NC>
 __device__ void routePoint(const StagedArgs &a, const nz_flash_out &out, int round, int64_t i, uint8_t stage,
@@ -177,6 +199,9 @@ stagedStartKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
     unsigned long long evals = 0;
     if (i < a.n)
     {
+        // final statuses overwrite this; a point a tripped self-check leaves keeps it
+        if (out.status)
+            out.status[i] = NZ_FLASH_UNFINISHED;
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
         Driver<NC> d;
         d.st = &states[i];
@@ -203,6 +228,8 @@ template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
 stagedClassifyKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int round)
 {
+    if (stagedTripped(a))
+        return;
     const int q = round & 1;
     const int count = a.counters[4 * round + 1];
     const int nseeds = seedCount<NC>(F);
@@ -239,6 +266,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                    const __grid_constant__ nz_flash_out out, int round, int which)
 {
+    if (stagedTripped(a))
+        return;
     const int count = which ? a.counters[kCounterSplit1] : a.counters[4 * round + 3];
     unsigned long long evals = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count && k < a.n; k += gridDim.x * blockDim.x)
@@ -279,6 +308,8 @@ template <int NC>
 __global__ void __launch_bounds__(kTrialBlock)
 stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
 {
+    if (stagedTripped(a))
+        return;
     const int queued = a.counters[kCounterThree];
     const long long total = queued < a.n ? queued : a.n;
     int *cursor = &a.counters[kCounterThreeCursor];
@@ -295,7 +326,7 @@ stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
     // a solve takes at most ssi + newton * (1 + 4 nc + 16) + tail steps (a few
     // hundred); the cap only guards against a wait that would never end
     long long guard = 0;
-    const long long guardMax = 1LL << 26;
+    const long long guardMax = F.spinLimit;
     while (true)
     {
         if (++guard > guardMax)
@@ -387,6 +418,8 @@ template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
 stagedThreeLongKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
 {
+    if (stagedTripped(a))
+        return;
     const int queued = a.counters[kCounterThreeLong];
     const int64_t count = queued < a.n ? queued : a.n;
     const int lane = threadIdx.x & 31;
@@ -442,6 +475,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedThreeResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                         const __grid_constant__ nz_flash_out out, int round)
 {
+    if (stagedTripped(a))
+        return;
     const int queued = a.counters[kCounterThree];
     const int count = queued < a.n ? queued : int(a.n);
     unsigned long long evals = 0;
@@ -469,6 +504,8 @@ template <int NC>
 __global__ void __launch_bounds__(kTrialBlock)
 stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int round)
 {
+    if (stagedTripped(a))
+        return;
     const int q = round & 1;
     const int nseeds = seedCount<NC>(F);
     const int ntasks = a.counters[4 * round];
@@ -487,7 +524,7 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
     // lanes' trials back to back, so this cap is far above any real need and
     // only guards against a wait that would never end.
     long long guard = 0;
-    const long long guardMax = 1LL << 26;
+    const long long guardMax = F.spinLimit;
     while (true)
     {
         if (++guard > guardMax)
@@ -638,6 +675,8 @@ template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
 stagedRr3MemoKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
 {
+    if (stagedTripped(a))
+        return;
     const int count = a.counters[kCounterFull];
     const int nseeds = seedCount<NC>(F);
     const int lane = threadIdx.x & 31;
@@ -744,6 +783,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedRecoverStartKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                          const __grid_constant__ nz_flash_out out)
 {
+    if (stagedTripped(a))
+        return;
     const int count = a.counters[kCounterFull];
     unsigned long long evals = 0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count && k < a.n; k += gridDim.x * blockDim.x)
@@ -786,6 +827,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedRecoverThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                          const __grid_constant__ nz_flash_out out)
 {
+    if (stagedTripped(a))
+        return;
     const int queued = a.counters[kCounterThree];
     const int count = queued < a.n ? queued : int(a.n);
     unsigned long long evals = 0;
@@ -831,6 +874,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedRecoverResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                           const __grid_constant__ nz_flash_out out, int rr)
 {
+    if (stagedTripped(a))
+        return;
     const int round = kMaxRounds + rr;
     const int q = round & 1;
     const int count = a.counters[4 * round + 1];
@@ -866,6 +911,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                  const __grid_constant__ nz_flash_out out)
 {
+    if (stagedTripped(a))
+        return;
     const int count = a.counters[kCounterRest];
     const int lane = threadIdx.x & 31;
     const int warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -950,6 +997,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int first,
                    int span)
 {
+    if (stagedTripped(a))
+        return;
     const int queued = a.counters[kCounterCont];
     const int64_t count = queued < a.contCap ? queued : a.contCap;
     const int lane = threadIdx.x & 31;
@@ -999,6 +1048,8 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedSelectKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                    const __grid_constant__ nz_flash_out out)
 {
+    if (stagedTripped(a))
+        return;
     const int queued = a.counters[kCounterCont];
     const int64_t count = queued < a.contCap ? queued : a.contCap;
     const int lane = threadIdx.x & 31;
@@ -1053,6 +1104,69 @@ stagedSelectKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
             }
             else if (accepted.converged)
                 writeFlashOut<NC>(out, a.n, i, accepted, NZ_FLASH_CONVERGED);
+        }
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
+// The mixed-precision form's last step: the FP64 ln-fugacity Newton polish
+// (Solver::polish) of every converged multiphase point, read back from and
+// written to the output record (it needs at least the presence, status,
+// fraction and composition arrays; fields the caller left out stay out).
+constexpr double kPolishTarget = 1.0e-11;   // largest ln-fugacity residual the polish aims for
+constexpr int kPolishSteps = 4;
+
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedPolishKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
+                   const __grid_constant__ nz_flash_out out)
+{
+    if (stagedTripped(a) || !out.status || !out.presence || !out.beta || !out.composition)
+        return;
+    unsigned long long evals = 0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n;
+         i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const uint8_t pres = out.presence[i];
+        if (out.status[i] != NZ_FLASH_CONVERGED || popcount3(pres) < 2)
+            continue;
+        Solver<NC> s;
+        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        double zn[NC];
+        for (int c = 0; c < NC; ++c)
+            zn[c] = a.z[c * a.n + i];
+        s.normalize(zn);
+        if (s.err)
+            continue;
+        Result<NC> r;
+        r.init();
+        r.converged = true;
+        r.presence = pres;
+        for (int p = 0; p < 3; ++p)
+        {
+            r.beta[p] = out.beta[p * a.n + i];
+            for (int c = 0; c < NC; ++c)
+                r.x[p][c] = out.composition[(p * NC + c) * a.n + i];
+        }
+        const bool replaced = s.polish(a.P[i], a.T[i], zn, r, kPolishTarget, kPolishSteps);
+        evals += s.evals;
+        if (!replaced)
+            continue;
+        for (int p = 0; p < 3; ++p)
+        {
+            if (out.saturation) out.saturation[p * a.n + i] = r.sat[p];
+            if (!(pres & bitOf(p)))
+                continue;
+            out.beta[p * a.n + i] = r.beta[p];
+            for (int c = 0; c < NC; ++c)
+                out.composition[(p * NC + c) * a.n + i] = r.x[p][c];
+            if (out.compressibility) out.compressibility[p * a.n + i] = r.Z[p];
+            if (out.molar_density) out.molar_density[p * a.n + i] = r.rho[p];
+        }
+        for (int c = 0; c < NC; ++c)
+        {
+            if (out.k_gas_oil) out.k_gas_oil[c * a.n + i] = r.Kg[c];
+            if (out.k_water_oil) out.k_water_oil[c * a.n + i] = r.Kw[c];
         }
     }
     warpAddEvals(a.evalCounter, evals);
@@ -1116,10 +1230,14 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
 
 // Launch sequence of one staged flash on `st`; the scratch block must hold
 // stagedScratchBytes<NC>(n) bytes.  No allocation, no host synchronisation.
+// `check` (null or two device ints) receives the batch's queue-bound and
+// spin-guard codes (0 = none tripped).  The mixed form ends with the FP64
+// ln-fugacity polish of its multiphase answers.
 template <int NC>
 int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
                  const double *z, const double *sal, const nz_flash_out &out,
-                 unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed = false)
+                 unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed = false,
+                 int *check = nullptr)
 {
     StagedArgs a = stagedCarve<NC>(scratch, n, F);
     a.mixed = mixed ? 1 : 0;
@@ -1129,9 +1247,9 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     a.sal = sal;
     a.evalCounter = evalCounter;
     cudaMemsetAsync(a.counters, 0, sizeof(int) * kCounterWords, st);
-    const bool check = stagedDebugSync();
+    const bool debugSync = stagedDebugSync();
     auto after = [&](const char *what, int round) {
-        if (!check)
+        if (!debugSync)
             return 0;
         cudaError_t e = cudaStreamSynchronize(st);
         int c[kCounterWords];
@@ -1184,6 +1302,9 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     stagedSelectKernel<NC><<<unsigned(smCount * 2), kFlashBlock, 0, st>>>(F, a, out);
     if (after("continuation", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the pressure continuation");
+    if (mixed)
+        stagedPolishKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
+    stagedCheckKernel<<<1, 32, 0, st>>>(a.counters, check);
     return 0;
 }
 

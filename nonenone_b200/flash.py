@@ -122,6 +122,17 @@ class CubicThreePhaseFlash(Context):
               "nz_flash_batch")
         return out
 
+    def self_check(self):
+        """(queue-bound code, spin-guard code) of the last staged batch, 0 when
+        none tripped; call after the batch's stream is synchronised."""
+        bound, guard = C.c_int32(), C.c_int32()
+        check(self.lib.nz_flash_check(self.handle, C.byref(bound), C.byref(guard)), "nz_flash_check")
+        return int(bound.value), int(guard.value)
+
+    def set_spin_limit(self, limit: int):
+        """Iteration cap of the staged kernels' lane-refill loops (default 2**26)."""
+        check(self.lib.nz_ctx_set_spin_limit(self.handle, int(limit)), "nz_ctx_set_spin_limit")
+
     def eos_eval_count(self) -> int:
         v = C.c_uint64()
         check(self.lib.nz_flash_eos_eval_count(self.handle, C.byref(v)), "nz_flash_eos_eval_count")
@@ -166,3 +177,41 @@ class CubicThreePhaseFlash(Context):
             _ptr(r["stable"]), _ptr(r["valid"]), _ptr(r["unstable_mask"]), _ptr(r["trial_sum"]),
             _ptr(r["incipient"]), _stream_ptr(stream)), "nz_stability_batch")
         return r
+
+
+def fugacity_residual(eos: "CubicEquationOfState", pressure, temperature, out, salinity=None,
+                      floor: float = 1.0e-20, chunk: int = 1 << 18):
+    """Largest |ln f_a - ln f_b| over the present phases of every converged
+    multiphase point of a flash answer `out` (the nz_flash_out dict of device
+    tensors), each phase's ln phi evaluated by the EOS entry point in its own
+    role; components below `floor` in either phase are skipped.  Returns a
+    float64 device tensor [n] with NaN at single-phase or failed points."""
+    d = eos.device
+    P = _dev(pressure, d)
+    T = _dev(temperature, d)
+    n = P.numel()
+    sal = _dev(salinity, d)
+    pres = out["presence"].to(torch.int64)
+    present = torch.stack([(pres >> p) & 1 for p in range(3)]).bool()
+    multi = (out["status"] == abi.FLASH_CONVERGED) & (present.sum(0) >= 2)
+    res = torch.full((n,), float("nan"), dtype=torch.float64, device=d)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        m = b - a
+        lnf = []
+        for p in range(3):
+            x = out["composition"][p][:, a:b].contiguous()
+            role = torch.full((m,), p, dtype=torch.int8, device=d)
+            _, lphi = eos.phase_result(P[a:b], T[a:b], x, role,
+                                       salinity=None if sal is None else sal[a:b])
+            lnf.append(lphi + torch.log(torch.clamp(x, min=1e-300)))
+        comp = out["composition"][:, :, a:b]
+        best = torch.zeros(m, dtype=torch.float64, device=d)
+        for p in range(3):
+            for q in range(p + 1, 3):
+                both = present[p, a:b] & present[q, a:b]
+                use = (comp[p] > floor) & (comp[q] > floor) & both[None, :]
+                diff = torch.where(use, (lnf[p] - lnf[q]).abs(), torch.zeros_like(lnf[p]))
+                best = torch.maximum(best, torch.nan_to_num(diff, nan=float("inf")).amax(0))
+        res[a:b] = torch.where(multi[a:b], best, res[a:b])
+    return res

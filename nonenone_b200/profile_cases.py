@@ -1,6 +1,6 @@
 """Single workloads to run under a profiler (one process, one GPU).
 
-  python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged]
+  python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged|mixed]
       one N-point batch of the seeded flash mixture (after a 4,096-point warm-up
       batch, so kernels of the measured batch come second)
   python -m nonenone_b200.profile_cases natural NX NY NZ [--update] [--per-cell]
@@ -22,7 +22,8 @@ def run_flash(n: int, precision: str) -> None:
     from . import abi, synth
     from .flash import CubicThreePhaseFlash
     from .fluids import make_fluid
-    prec = abi.PRECISION_FP64 if precision == "fp64" else abi.PRECISION_FP64_STAGED
+    prec = {"fp64": abi.PRECISION_FP64, "fp64_staged": abi.PRECISION_FP64_STAGED,
+            "mixed": abi.PRECISION_MIXED}[precision]
     fl = CubicThreePhaseFlash(make_fluid())
     P, T, z = synth.flash_points(n, seed=1)
     fl.flash(P[:4096], T[:4096], np.ascontiguousarray(z[:, :4096]), precision=prec)
@@ -72,8 +73,22 @@ def run_natural(nx: int, ny: int, nz: int, update: bool = False, per_cell: bool 
         nat.form_function(primary, ps, out=F)
         nat.assemble_jacobian(primary, ps, values=vals)
     torch.cuda.synchronize()
+    times = {"residual": [], "jacobian": []}
+    for _ in range(5):
+        for key, fn in (("residual", lambda: nat.form_function(primary, ps, out=F)),
+                        ("jacobian", lambda: nat.assemble_jacobian(primary, ps, values=vals))):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            times[key].append(a.elapsed_time(b))
+    jac_ms = sorted(times["jacobian"])[2]
+    gb = (vals.numel() + F.numel()) * 8 / 1e9
     print(f"natural {nx}x{ny}x{nz}: {grid.ncell} cells, {nat.nnzb} blocks, "
-          f"{vals.numel() * 8 / 1e9:.3f} GB of Jacobian values")
+          f"{vals.numel() * 8 / 1e9:.3f} GB of Jacobian values; residual {sorted(times['residual'])[2]:.3f} ms, "
+          f"jacobian {jac_ms:.3f} ms = {gb / (jac_ms * 1e-3):.0f} GB/s; "
+          f"checksum {float(vals.abs().sum()):.12e}")
 
 
 def main(argv=None) -> int:
@@ -81,7 +96,7 @@ def main(argv=None) -> int:
     sub = ap.add_subparsers(dest="case", required=True)
     f = sub.add_parser("flash")
     f.add_argument("n", type=int)
-    f.add_argument("--precision", default="fp64_staged", choices=["fp64", "fp64_staged"])
+    f.add_argument("--precision", default="fp64_staged", choices=["fp64", "fp64_staged", "mixed"])
     nat = sub.add_parser("natural")
     nat.add_argument("nx", type=int)
     nat.add_argument("ny", type=int)

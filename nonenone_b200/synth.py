@@ -10,6 +10,9 @@ Batched P-T-z flash (1,048,576 points, nc=3 H2O/CO2/nC10):
     23 % "3ph"   P ~ U[5,12] MPa, T ~ U[340,423] K, z ~ Dir(2,2,0.6) -> 73 % 3-ph
   which gives roughly 40 % / 40 % / 20 % single / two / three-phase.
   Soreide-Whitson points add salinity ~ U[0,2] mol/kg.
+  benchmark_points adds the 5 % slice of points next to a phase boundary
+  (boundary_points: P bisected to a label change, then offset by <= 5e-6
+  relative).
 """
 from __future__ import annotations
 
@@ -50,6 +53,76 @@ def flash_points(n: int, seed: int = 1, salinity: bool = False):
     if salinity:
         return P, T, Z, rng.uniform(0.0, 2.0, n)
     return P, T, Z
+
+
+BOUNDARY_FRACTION = 0.05
+
+
+def boundary_points(n: int, labels, seed: int = 7, salinity: bool = False, offset=(1.0e-10, 5.0e-6),
+                    bisections: int = 44):
+    """n points next to a phase boundary (the benchmark's "5 % within
+    |TPD| < 1e-6" slice): for (T, z) drawn from the raw box, P is bisected
+    between 5 and 40 MPa on a change of the phase label, then moved off the
+    boundary by a relative offset of either sign and log-uniform magnitude in
+    `offset` (for the H2O/CO2/nC10 fluid the |TPD| of the boundary phase then
+    lies between ~1e-12 and ~1e-6, a fraction of the points below 1e-8).
+
+    `labels(P, T, z, salinity)` returns the phase-presence labels of a batch
+    (any flash: the oracle when fixtures are made, the GPU flash when the
+    benchmark builds its batch; 0 = not converged).  (T, z) pairs whose label
+    does not change between 5 and 40 MPa, or whose bracket meets a flash that
+    fails, are redrawn: the boundary sought is between two answered phase
+    sets, not the edge of the flash's convergence region.  Returns P, T,
+    z[3, n] (and salinity)."""
+    rng = np.random.default_rng(seed)
+    Ps, Ts, Zs, Ss = [], [], [], []
+    have = 0
+    while have < n:
+        m = max(2 * (n - have), 64)
+        T = rng.uniform(303.0, 423.0, m)
+        z = np.ascontiguousarray(rng.dirichlet([2.0, 1.0, 1.0], m).T)
+        sal = rng.uniform(0.0, 2.0, m) if salinity else None
+        lo = np.full(m, 5.0e6)
+        hi = np.full(m, 40.0e6)
+        lab_lo = labels(lo, T, z, sal)
+        lab_hi = labels(hi, T, z, sal)
+        keep = (lab_lo != lab_hi) & (lab_lo != 0) & (lab_hi != 0)
+        lo, hi, T, z, lab_lo = lo[keep], hi[keep], T[keep], np.ascontiguousarray(z[:, keep]), lab_lo[keep]
+        sal = None if sal is None else sal[keep]
+        answered = np.ones(lo.size, bool)
+        for _ in range(bisections):
+            mid = 0.5 * (lo + hi)
+            lab = labels(mid, T, z, sal)
+            answered &= lab != 0
+            same = lab == lab_lo
+            lo = np.where(same, mid, lo)
+            hi = np.where(same, hi, mid)
+        mag = 10.0 ** rng.uniform(np.log10(offset[0]), np.log10(offset[1]), lo.size)
+        P = 0.5 * (lo + hi) * (1.0 + np.where(rng.uniform(size=lo.size) < 0.5, -mag, mag))
+        P, T, z = P[answered], T[answered], np.ascontiguousarray(z[:, answered])
+        sal = None if sal is None else sal[answered]
+        take = min(P.size, n - have)
+        Ps.append(P[:take])
+        Ts.append(T[:take])
+        Zs.append(z[:, :take])
+        if sal is not None:
+            Ss.append(sal[:take])
+        have += take
+    P, T, Z = np.concatenate(Ps), np.concatenate(Ts), np.ascontiguousarray(np.concatenate(Zs, axis=1))
+    if salinity:
+        return P, T, Z, np.concatenate(Ss)
+    return P, T, Z
+
+
+def benchmark_points(n: int, boundary, seed: int = 1):
+    """The batched-flash benchmark's batch: the label mixture of flash_points
+    for n - len(boundary) points and the given near-boundary slice
+    (boundary_points output, ~5 %) for the rest, shuffled together."""
+    nb = boundary[0].shape[0]
+    mix = flash_points(n - nb, seed=seed)
+    perm = np.random.default_rng(seed + 104729).permutation(n)
+    return tuple(np.ascontiguousarray(np.concatenate([a, b], axis=a.ndim - 1)[..., perm])
+                 for a, b in zip(mix, boundary))
 
 
 def raw_box_points(n: int, seed: int = 12345):

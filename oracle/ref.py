@@ -37,6 +37,7 @@ def lib():
         L.nzref_eos_phase_batch.argtypes = [vp, i64, vp, vp, vp, vp, vp, vp, vp]
         L.nzref_stability_batch.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, vp,
                                             vp, vp, vp, vp, vp, i32]
+        L.nzref_boundary_distance.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, i32]
         L.nzref_natural_create.argtypes = [vp, vp]
         L.nzref_natural_create.restype = vp
         L.nzref_natural_destroy.argtypes = [vp]
@@ -85,6 +86,32 @@ def flash_batch(fluid, P, T, z, salinity=None, options=None, threads=1):
     _check(lib().nzref_flash_batch(C.byref(fluid), C.byref(opts), n, _p(P), _p(T),
                                    _p(z), _p(sal), C.byref(fo), int(threads)))
     return out
+
+
+def boundary_distance(fluid, P, T, z, out, salinity=None, options=None, threads=8):
+    """Distance of converged flash answers from a phase boundary in |TPD|:
+    0 when a present phase has a fraction below 1e-8 (it is appearing or
+    vanishing: its tangent-plane distance is zero), else the smallest
+    |1 - trialSum| over the non-trivial stationary points of the reference's
+    stability trials for the missing phases (inf when there is none; NaN when
+    the trials throw).  Points that did not converge, and three-phase points
+    without a small phase, get inf."""
+    nc = fluid.nc
+    P = np.ascontiguousarray(P, dtype=np.float64)
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    n = P.shape[0]
+    z = np.ascontiguousarray(z, dtype=np.float64).reshape(nc, n)
+    pres = np.ascontiguousarray(np.where(out["status"] == 0, out["presence"], 0), dtype=np.uint8)
+    comps = np.ascontiguousarray(out["composition"], dtype=np.float64).reshape(3, nc, n)
+    sal = None if salinity is None else np.ascontiguousarray(salinity, dtype=np.float64)
+    dist = np.zeros(n)
+    opts = options if options is not None else default_flash_options()
+    _check(lib().nzref_boundary_distance(C.byref(fluid), C.byref(opts), n, _p(P), _p(T), _p(z), _p(sal),
+                                         _p(pres), _p(comps), _p(dist), int(threads)))
+    present = np.stack([(pres >> p) & 1 for p in range(3)]).astype(bool)
+    small = np.any(present & (np.asarray(out["beta"]) < 1.0e-8), axis=0)
+    dist[small] = 0.0
+    return dist
 
 
 def eos_phase_batch(fluid, P, T, x, role, salinity=None):

@@ -14,6 +14,8 @@
 //                               + natural_petsc_runtime_cell_cache.inc:8-185
 //   * assembleJacobian_      -> natural_petsc_runtime_jacobian.inc:8-299
 //   * previous accumulation  -> natural_petsc_runtime_cache_history.inc:180-262
+//   * boundary distance      -> the trial loop of stabilityTest
+//                               (three_phase_flash.hpp:399-480), non-trivial trials only
 // Every physical computation is a call into the reference's own headers.
 #include <indices/indices.hpp>
 #include <natural/fluid_system.hpp>
@@ -29,6 +31,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -703,9 +706,131 @@ int dispatchNc(int nc, Args &&...args)
     }
 }
 
+// ---- boundary distance of a converged flash answer (|TPD| of its missing
+// phases).  stabilityTest reports the largest trial sum of each missing phase,
+// which is exactly 1 whenever a trial falls back onto an existing phase (a
+// trivial stationary point), so it cannot say how far a point is from the
+// boundary.  This restates stabilityTest's trial loop
+// (three_phase_flash.hpp:399-480) with the reference's own seed list and
+// trial solver, keeping only the non-trivial trials that do not coincide with
+// an active phase: distance = min over missing phases of |1 - best such sum|
+// (infinite when no such stationary point exists).  The private members are
+// reached through the standard explicit-instantiation access rule.
+template <int NC>
+struct TrialAccess
+{
+    friend auto trialFn(TrialAccess<NC>);
+    friend auto seedsFn(TrialAccess<NC>);
+    friend auto phaseFn(TrialAccess<NC>);
+};
+template <int NC, auto Trial, auto Seeds, auto Phase>
+struct TrialRob
+{
+    friend auto trialFn(TrialAccess<NC>) { return Trial; }
+    friend auto seedsFn(TrialAccess<NC>) { return Seeds; }
+    friend auto phaseFn(TrialAccess<NC>) { return Phase; }
+};
+#define NZ_TRIAL_ROB(NCV)                                                                              \
+    template struct TrialRob<NCV, &CubicThreePhaseFlash<SIdx<NCV>>::stabilityTrial_,                  \
+                             &CubicThreePhaseFlash<SIdx<NCV>>::stabilitySeeds_,                      \
+                             &CubicThreePhaseFlash<SIdx<NCV>>::phaseResult_>;
+NZ_TRIAL_ROB(2)
+NZ_TRIAL_ROB(3)
+NZ_TRIAL_ROB(4)
+NZ_TRIAL_ROB(5)
+NZ_TRIAL_ROB(6)
+NZ_TRIAL_ROB(8)
+#undef NZ_TRIAL_ROB
+
+template <int NC>
+int boundaryBatch(const nz_fluid_desc *d, const nz_flash_options *o, int64_t n, const double *P,
+                  const double *T, const double *z, const double *salinity, const uint8_t *presence,
+                  const double *comps, double *distance, int threads)
+{
+    using I = SIdx<NC>;
+    using Flash = CubicThreePhaseFlash<I>;
+    const auto options = toOptions(o, d->water_component);
+    const auto trialOf = trialFn(TrialAccess<NC>{});
+    const auto seedsOf = seedsFn(TrialAccess<NC>{});
+    const auto phaseOf = phaseFn(TrialAccess<NC>{});
+    const CompositionalPhase phases[3] = {CompositionalPhase::Oil, CompositionalPhase::Gas,
+                                          CompositionalPhase::Water};
+    parallelFor(n, threads, [&](int64_t b, int64_t e, int) {
+        for (int64_t i = b; i < e; ++i)
+        {
+            distance[i] = std::numeric_limits<double>::infinity();
+            const uint8_t active = presence[i];
+            if (active == 0 || active == 7)
+                continue;
+            const auto eos = makeEos<I>(*d, salinity ? salinity[i] : d->sw_salinity);
+            Flash flash(eos, options);
+            std::array<double, NC> zi{};
+            std::array<std::array<double, NC>, 3> x{};
+            double zs = 0.0;
+            for (int c = 0; c < NC; ++c)
+                zs += (zi[c] = z[c * n + i]);
+            for (int c = 0; c < NC; ++c)
+                zi[c] /= zs;
+            for (int p = 0; p < 3; ++p)
+            {
+                double s = 0.0;
+                for (int c = 0; c < NC; ++c)
+                    s += (x[p][c] = comps[(p * NC + c) * n + i]);
+                if (active & (1u << p))
+                    for (int c = 0; c < NC; ++c)
+                        x[p][c] /= s;
+            }
+            int ref = 0;
+            while (!(active & (1u << ref)))
+                ++ref;
+            try
+            {
+                const auto refThermo = (flash.*phaseOf)(phases[ref], P[i], T[i], x[ref]);
+                std::array<double, NC> logReference{};
+                for (int c = 0; c < NC; ++c)
+                    logReference[c] = std::log(std::max(x[ref][c], options.compositionFloor)) +
+                                      std::log(std::max(refThermo.fugacityCoefficient[c], 1.0e-300));
+                const double coincidence = std::max(10.0 * options.coincidentPhaseCompositionTolerance, 1.0e-7);
+                double dist = std::numeric_limits<double>::infinity();
+                for (int p = 0; p < 3; ++p)
+                {
+                    if (active & (1u << p))
+                        continue;
+                    const auto seeds = (flash.*seedsOf)(phases[p], P[i], T[i], zi, x[ref]);
+                    for (std::size_t k = 0; k < seeds.size; ++k)
+                    {
+                        const auto t = (flash.*trialOf)(phases[p], P[i], T[i], logReference, x[ref], seeds.values[k]);
+                        if (!t.valid || t.trivial)
+                            continue;
+                        bool coincides = false;
+                        for (int q = 0; q < 3 && !coincides; ++q)
+                        {
+                            if (!(active & (1u << q)))
+                                continue;
+                            double m = 0.0;
+                            for (int c = 0; c < NC; ++c)
+                                m = std::max(m, std::abs(t.composition[c] - x[q][c]));
+                            coincides = m <= coincidence;
+                        }
+                        if (!coincides)
+                            dist = std::min(dist, std::abs(1.0 - t.sum));
+                    }
+                }
+                distance[i] = dist;
+            }
+            catch (const std::exception &)
+            {
+                distance[i] = std::numeric_limits<double>::quiet_NaN();
+            }
+        }
+    });
+    return NZ_OK;
+}
+
 template <int NC> struct FlashRun { template <class... A> static int run(A &&...a) { return flashBatch<NC>(std::forward<A>(a)...); } };
 template <int NC> struct EosRun { template <class... A> static int run(A &&...a) { return eosBatch<NC>(std::forward<A>(a)...); } };
 template <int NC> struct StabRun { template <class... A> static int run(A &&...a) { return stabilityBatch<NC>(std::forward<A>(a)...); } };
+template <int NC> struct BoundaryRun { template <class... A> static int run(A &&...a) { return boundaryBatch<NC>(std::forward<A>(a)...); } };
 
 template <class F>
 int guarded(F &&f)
@@ -750,6 +875,16 @@ int nzref_stability_batch(const nz_fluid_desc *d, const nz_flash_options *o, int
     return guarded([&] {
         return dispatchNc<StabRun>(d->nc, d, o, n, P, T, z, salinity, active, comps,
                                    stable, valid, unstableMask, trialSum, incipient, threads);
+    });
+}
+
+int nzref_boundary_distance(const nz_fluid_desc *d, const nz_flash_options *o, int64_t n,
+                            const double *P, const double *T, const double *z,
+                            const double *salinity, const uint8_t *presence,
+                            const double *comps, double *distance, int threads)
+{
+    return guarded([&] {
+        return dispatchNc<BoundaryRun>(d->nc, d, o, n, P, T, z, salinity, presence, comps, distance, threads);
     });
 }
 

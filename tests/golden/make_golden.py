@@ -10,16 +10,19 @@ reference's own FP64 C++ (oracle/_ref/libnzref.so); the inputs are seeded
   flash_pr_nc6.npz  512 points, six components, PR
   flash_cpa_nc3.npz 1024 points, PR-CPA H2O/CO2/nC10 of the reference's 60x20 case
                     (4C water, CO2 one acceptor site: the single-donor path)
+  flash_boundary_pr_nc3.npz  512 points next to a phase boundary
+                    (synth.boundary_points with the reference's own labels): the
+                    benchmark's near-boundary slice
+  flash_boundary_sw_nc3.npz  256 such points, Soreide-Whitson, salinity ~ U[0,2]
   flash_continuation_pr_nc3.npz  192 points of the 1,048,576-point bench batch
                     (synth.flash_points(2**20, seed=1)) that reach the flash's last
                     fallback, the pressure continuation: 160 it rescues and 32 it
                     does not (RESCUED / FAILING below, found by scanning the batch
                     with this library's host-compiled solver with the continuation
                     switched off; only the choice of inputs comes from that scan)
-Each holds the inputs, the full nz_flash_out record, and for converged
-points the stability trial sums of the missing phases of the final state
-(|trialSum - 1| is the distance to the phase boundary used to exclude
-boundary points from label comparisons).
+Each holds the inputs, the full nz_flash_out record and, per point, the
+distance of the reference's answer from a phase boundary in |TPD|
+(tpd_distance; label comparisons exclude points below 1e-8).
 """
 from __future__ import annotations
 
@@ -60,22 +63,10 @@ FAILING = (
 
 
 def boundary_distance(fluid, P, T, z, out, salinity=None):
-    """min over missing phases of |trialSum - 1| for converged points (inf otherwise)."""
-    n = P.shape[0]
-    dist = np.full(n, np.inf)
-    ok = (out["status"] == abi.FLASH_CONVERGED) & (out["presence"] != 7) & (out["presence"] != 0)
-    idx = np.where(ok)[0]
-    if idx.size == 0:
-        return dist
-    st = ref.stability_batch(fluid, P[idx], T[idx], z[:, idx], out["presence"][idx],
-                             out["composition"][:, :, idx],
-                             None if salinity is None else salinity[idx], threads=8)
-    ts = st["trial_sum"]
-    for k, i in enumerate(idx):
-        pres = out["presence"][i]
-        d = [abs(ts[p, k] - 1.0) for p in range(3) if not (pres >> p) & 1]
-        dist[i] = min(d) if d else np.inf
-    return dist
+    """|TPD| distance of each converged answer from a phase boundary
+    (oracle.ref.boundary_distance: non-trivial stability trials of the missing
+    phases, zero for a present phase below a fraction of 1e-8)."""
+    return ref.boundary_distance(fluid, P, T, z, out, salinity)
 
 
 def make(name, fluid, P, T, z, salinity=None):
@@ -107,6 +98,12 @@ def main():
     make("flash_pr_nc6.npz", six, P, T, z)
     P, T, z = synth.flash_points(1024, seed=104)
     make("flash_cpa_nc3.npz", make_cpa_h2o_co2_nc10(), P, T, z)
+    labels = lambda P, T, z, s, f=pr: ref.flash_batch(f, P, T, z, salinity=s, threads=8)["presence"]
+    P, T, z = synth.boundary_points(512, labels, seed=105)
+    make("flash_boundary_pr_nc3.npz", pr, P, T, z)
+    labels = lambda P, T, z, s, f=sw: ref.flash_batch(f, P, T, z, salinity=s, threads=8)["presence"]
+    P, T, z, s = synth.boundary_points(256, labels, seed=106, salinity=True)
+    make("flash_boundary_sw_nc3.npz", sw, P, T, z, s)
     P, T, z = synth.flash_points(1 << 20, seed=1)
     sel = np.array(RESCUED + FAILING)
     make("flash_continuation_pr_nc3.npz", pr, P[sel], T[sel], np.ascontiguousarray(z[:, sel]))
