@@ -22,6 +22,8 @@
  *                        (natural_petsc_runtime_residual.inc:19-133)
  *   nz_jacobian          NaturalPetscRuntime::assembleJacobian_
  *                        (natural_petsc_runtime_jacobian.inc:8-109,120-299)
+ *   nz_jacobian_columns  the same, in the per-cell column order of its
+ *                        MatSetValuesBlocked calls (jacobian.inc:279-299)
  *   nz_natural_init_ptz  NaturalPetscRuntime::initializeUniformFromPTZ
  *                        (natural_petsc_runtime_state.inc:107-164), per cell
  *   nz_natural_pattern   buildNaturalJacobianPattern
@@ -353,6 +355,17 @@ int nz_residual(nz_natural* nat, const double* primary,
 int nz_jacobian(nz_natural* nat, const double* primary,
                 const double* phase_state, double* baij_values,
                 double* residual, void* stream);
+/* The same values in cell-column order, for the reference's batched block
+ * write (insertPreparedCellJacobianColumn_, natural_petsc_runtime_jacobian.inc:
+ * 279-299): cell c's column is the contiguous run of 1 + nconn(c) blocks that
+ * starts at block c + conn_offset[c] -- the self block, then the block of each
+ * of its connections in connection order -- i.e. exactly the values of
+ *   MatSetValuesBlocked(J, 1 + nconn(c), rows, 1, &c, vals, ADD_VALUES)
+ * with rows = {c, conn_neighbor[conn_offset[c] .. conn_offset[c+1])}.
+ * column_values holds nnzb * B * B doubles; residual may be NULL. */
+int nz_jacobian_columns(nz_natural* nat, const double* primary,
+                        const double* phase_state, double* column_values,
+                        double* residual, void* stream);
 
 /* ---- diagnostics -------------------------------------------------------------
  * Measured FMA throughput of the FP64 and FP32 CUDA-core pipes of `device`

@@ -3585,22 +3585,57 @@ struct Solver
     // the flash's own residual (evalTwo / evalThree: Rachford-Rice inside) and
     // a forward-difference Jacobian, until the largest residual is below
     // `target` or `maxSteps` steps are done.  `r` is replaced only by a state
-    // with the same phases and a smaller residual; an error inside leaves `r`
-    // and `err` as they were.  Returns true when `r` was replaced.
-    NZ_HDN bool polish(double P, double T, const double *z, Result<NC> &r, double target, int maxSteps)
+    // with the same phases, a smaller residual and values within `maxChange`
+    // of r's; an error inside leaves `r` and `err` as they were.  Returns true
+    // when `r` was replaced.
+    NZ_HDN bool polish(double P, double T, const double *z, Result<NC> &r, double target, int maxSteps,
+                       double maxChange = 1.0e-8)
     {
         if (!r.converged)
             return false;
         const int errBefore = err;
         err = ERR_NONE;
         bool replaced = false;
+        Result<NC> q = r;
         const int count = popcount3(r.presence);
         if (count == 2)
-            replaced = polishTwo(P, T, z, r, target, maxSteps);
+            replaced = polishTwo(P, T, z, q, target, maxSteps);
         else if (count == 3)
-            replaced = polishThree(P, T, z, r, target, maxSteps);
+            replaced = polishThree(P, T, z, q, target, maxSteps);
         err = errBefore;
-        return replaced;
+        if (!replaced)
+            return false;
+        // A converged answer is within its own tolerance of the exact one; a
+        // polish that moves a fraction or a mole fraction further than
+        // maxChange (relative to max(1, |v|)) has found a different, badly
+        // conditioned solution next to a phase boundary: keep the answer.
+        double change = 0.0;
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+        {
+            if (!(r.presence & bitOf(p)))
+                continue;
+            change = smax(change, fabs(q.beta[p] - r.beta[p]) / smax(1.0, fabs(r.beta[p])));
+#pragma unroll
+            for (int i = 0; i < NC; ++i)
+                change = smax(change, fabs(q.x[p][i] - r.x[p][i]) / smax(1.0, fabs(r.x[p][i])));
+        }
+        if (!(change <= maxChange))
+            return false;
+        r = q;
+        return true;
+    }
+
+    // The answer's phases evaluate, in their slots' roles, to the
+    // compressibilities the answer records: the polish works in those roles
+    // (an answer of the SW role search that does not has other roles or roots).
+    NZ_HD bool sameRoots(const Result<NC> &r, const Result<NC> &e) const
+    {
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+            if ((r.presence & bitOf(p)) && !(fabs(e.Z[p] - r.Z[p]) <= 1.0e-6 * smax(1.0, fabs(r.Z[p]))))
+                return false;
+        return true;
     }
 
     NZ_HDN bool polishTwo(double P, double T, const double *z, Result<NC> &r, double target, int maxSteps)
@@ -3613,7 +3648,7 @@ struct Solver
             logK[i] = log(smax(r.x[second][i], O().floor) / smax(r.x[first][i], O().floor));
         TwoPhaseLogKState<NC> base, probe;
         evalTwo(P, T, z, first, second, logK, r.beta[second], base);
-        if (!base.valid || err)
+        if (!base.valid || err || !sameRoots(r, base.result))
             return false;
         const double start = base.norm;
         bool moved = false;
@@ -3629,9 +3664,18 @@ struct Solver
 #pragma unroll
                 for (int i = 0; i < NC; ++i)
                     pert[i] = logK[i];
-                const double h = O().fdStep * smax(1.0, fabs(logK[col]));
-                pert[col] += h;
+                // forward difference, backward where the forward probe leaves the
+                // admissible fractions (a small phase close to zero)
+                double h = O().fdStep * smax(1.0, fabs(logK[col]));
+                pert[col] = logK[col] + h;
                 evalTwo(P, T, z, first, second, pert, base.result.beta[second], probe);
+                if (!probe.valid || err)
+                {
+                    err = ERR_NONE;
+                    h = -h;
+                    pert[col] = logK[col] + h;
+                    evalTwo(P, T, z, first, second, pert, base.result.beta[second], probe);
+                }
                 ok = probe.valid && !err;
                 if (ok)
 #pragma unroll
@@ -3703,7 +3747,7 @@ struct Solver
         }
         ThreePhaseLogKState<NC> base, probe;
         evalThree(P, T, z, logK, r.beta[1], r.beta[2], base);
-        if (!base.valid || err)
+        if (!base.valid || err || !sameRoots(r, base.result))
             return false;
         const double start = base.norm;
         bool moved = false;
@@ -3719,9 +3763,16 @@ struct Solver
 #pragma unroll
                 for (int i = 0; i < M; ++i)
                     pert[i] = logK[i];
-                const double h = O().fdStep * smax(1.0, fabs(logK[col]));
-                pert[col] += h;
+                double h = O().fdStep * smax(1.0, fabs(logK[col]));
+                pert[col] = logK[col] + h;
                 evalThree(P, T, z, pert, base.result.beta[1], base.result.beta[2], probe);
+                if (!probe.valid || err)
+                {
+                    err = ERR_NONE;
+                    h = -h;
+                    pert[col] = logK[col] + h;
+                    evalThree(P, T, z, pert, base.result.beta[1], base.result.beta[2], probe);
+                }
                 ok = probe.valid && !err;
                 if (ok)
 #pragma unroll

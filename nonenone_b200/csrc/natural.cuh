@@ -51,7 +51,21 @@ struct NatGeom
     const int64_t *connSlot;   // [nconn] block index of (neighbor, c)
     const double *prevAcc;     // [ncell][NC] accumulation of the accepted state
     double *cache;             // [fields][ncell] frozen exterior values
+    int columnOrder;           // Jacobian output: 0 pattern (block-row) order, 1 cell-column order
 };
+
+// Block index of a Jacobian block in the output array.  Pattern order: the
+// BAIJ slot of (c, c) / (neighbor, c).  Cell-column order: cell c's column
+// -- its self block, then the block of each connection in connection order --
+// is one contiguous run of 1 + nconn(c) blocks starting at c + offset[c].
+NZ_BOTH int64_t selfBlock(const NatGeom &g, int64_t c)
+{
+    return g.columnOrder ? c + g.offset[c] : g.selfSlot[c];
+}
+NZ_BOTH int64_t connBlock(const NatGeom &g, int64_t c, int64_t j)
+{
+    return g.columnOrder ? c + j + 1 : g.connSlot[j];
+}
 
 // Primary / equation indices of the fully compositional layout without wells
 // (indices/include/indices/indices.hpp:30-45).

@@ -174,7 +174,7 @@ NZ_HD bool cellJacobianColumn(const FluidDev &F, const NatConst &K, const NatGeo
         loadSide<NC>(g.cache, g.ncell, nb, ex);
         Dual flux[NC];
         faceFlux<NC, Dual>(st, pr, ex, g.trans[j], g.gravity[j], g.volume[c], g.volume[nb], c, nb, flux);
-        double *recip = values + g.connSlot[j] * (B * B);
+        double *recip = values + connBlock(g, c, j) * (B * B);
         for (int r = 0; r < B; ++r)
             recip[r * B + k] = r < NC ? -flux[r].d : 0.0;
         for (int i = 0; i < NC; ++i)
@@ -187,7 +187,7 @@ NZ_HD bool cellJacobianColumn(const FluidDev &F, const NatConst &K, const NatGeo
                 outward[i] += fv[i];
         }
     }
-    double *self = values + g.selfSlot[c] * (B * B);
+    double *self = values + selfBlock(g, c) * (B * B);
     for (int r = 0; r < B; ++r)
         self[r * B + k] = res[r].d;
     if (wantResidual)
@@ -450,17 +450,21 @@ __global__ void __launch_bounds__(kNatBlock) natJacobianKernelN(const __grid_con
         maxFaces = max(maxFaces, __shfl_xor_sync(0xffffffffu, maxFaces, off));
     double *myTile = tile + (group < perWarp ? group : 0) * BB;
 
-    // store the tiles of the warp's cells that have a block in this pass
+    // store the tiles of the warp's cells that have a block in this pass; the
+    // loop runs the same number of times on every lane (the tiles' total need
+    // not be a multiple of 32), so every shuffle has the whole warp
     auto flush = [&](bool has, int64_t slot) {
         __syncwarp();
-        for (int e = lane; e < perWarp * BB; e += 32)
+        constexpr int total = perWarp * BB;
+        for (int base = 0; base < total; base += 32)
         {
-            const int q = e / BB;
+            const int e = base + lane;
+            const int q = e < total ? e / BB : 0;
             const int o = e - q * BB;
             const int owner = q * G;
             const int qHas = __shfl_sync(0xffffffffu, int(has), owner);
             const long long qSlot = __shfl_sync(0xffffffffu, (long long)slot, owner);
-            if (qHas)
+            if (e < total && qHas)
                 values[qSlot * BB + o] = tile[e];
         }
         __syncwarp();
@@ -485,7 +489,7 @@ __global__ void __launch_bounds__(kNatBlock) natJacobianKernelN(const __grid_con
                 for (int jj = 0; jj < KD; ++jj)
                     if (k0 + jj < B)
                         myTile[r * B + k0 + jj] = r < NC ? -flux[r].d[jj] : 0.0;
-            slot = g.connSlot[j];
+            slot = connBlock(g, c, j);
             if (wantResidual)
             {
                 double fv[NC];
@@ -501,7 +505,7 @@ __global__ void __launch_bounds__(kNatBlock) natJacobianKernelN(const __grid_con
             for (int jj = 0; jj < KD; ++jj)
                 if (k0 + jj < B)
                     myTile[r * B + k0 + jj] = res[r].d[jj];
-    flush(ok, ok ? g.selfSlot[c] : 0);
+    flush(ok, ok ? selfBlock(g, c) : 0);
     if (wantResidual)
     {
         for (int i = 0; i < NC; ++i)

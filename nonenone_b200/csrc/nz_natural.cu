@@ -595,27 +595,40 @@ int nz_residual(nz_natural *nat, const double *primary, const double *phase_stat
     return syncFlag(nat, st, "nz_residual");
 }
 
-int nz_jacobian(nz_natural *nat, const double *primary, const double *phase_state, double *baij_values,
-                double *residual, void *stream)
+static int jacobianInOrder(nz_natural *nat, const double *primary, const double *phase_state, double *values,
+                           double *residual, void *stream, int columnOrder, const char *what)
 {
-    if (!nat || !primary || !phase_state || !baij_values)
-        return setError(NZ_ERR_ARGUMENT, "nz_jacobian: null argument");
+    if (!nat || !primary || !phase_state || !values)
+        return setError(NZ_ERR_ARGUMENT, "%s: null argument", what);
     if (!nat->historySet)
-        return setError(NZ_ERR_ARGUMENT, "nz_jacobian: call nz_natural_set_history first");
+        return setError(NZ_ERR_ARGUMENT, "%s: call nz_natural_set_history first", what);
     cudaSetDevice(nat->ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(nat->flag, 0, sizeof(int), st);
     if (e != cudaSuccess)
-        return cudaFail(e, "nz_jacobian");
+        return cudaFail(e, what);
     NatLaunch a = nat->launchArgs(primary, phase_state);
-    a.values = baij_values;
+    a.values = values;
     a.residual = residual;
     int rc = natDispatch(nat->nc, NAT_CACHE, a, st);
+    a.g.columnOrder = columnOrder;
     if (rc == NZ_OK)
         rc = natDispatch(nat->nc, NAT_JACOBIAN, a, st);
     if (rc != NZ_OK)
         return rc;
-    return syncFlag(nat, st, "nz_jacobian");
+    return syncFlag(nat, st, what);
+}
+
+int nz_jacobian(nz_natural *nat, const double *primary, const double *phase_state, double *baij_values,
+                double *residual, void *stream)
+{
+    return jacobianInOrder(nat, primary, phase_state, baij_values, residual, stream, 0, "nz_jacobian");
+}
+
+int nz_jacobian_columns(nz_natural *nat, const double *primary, const double *phase_state, double *column_values,
+                        double *residual, void *stream)
+{
+    return jacobianInOrder(nat, primary, phase_state, column_values, residual, stream, 1, "nz_jacobian_columns");
 }
 
 } // extern "C"

@@ -1112,7 +1112,8 @@ stagedSelectKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
 // The mixed-precision form's last step: the FP64 ln-fugacity Newton polish
 // (Solver::polish) of every converged multiphase point, read back from and
 // written to the output record (it needs at least the presence, status,
-// fraction and composition arrays; fields the caller left out stay out).
+// fraction, composition and compressibility arrays; fields the caller left
+// out stay out).
 constexpr double kPolishTarget = 1.0e-11;   // largest ln-fugacity residual the polish aims for
 constexpr int kPolishSteps = 4;
 
@@ -1121,7 +1122,7 @@ __global__ void __launch_bounds__(kFlashBlock)
 stagedPolishKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
                    const __grid_constant__ nz_flash_out out)
 {
-    if (stagedTripped(a) || !out.status || !out.presence || !out.beta || !out.composition)
+    if (stagedTripped(a) || !out.status || !out.presence || !out.beta || !out.composition || !out.compressibility)
         return;
     unsigned long long evals = 0;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.n;
@@ -1145,6 +1146,7 @@ stagedPolishKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
         for (int p = 0; p < 3; ++p)
         {
             r.beta[p] = out.beta[p * a.n + i];
+            r.Z[p] = out.compressibility[p * a.n + i];
             for (int c = 0; c < NC; ++c)
                 r.x[p][c] = out.composition[(p * NC + c) * a.n + i];
         }

@@ -20,7 +20,7 @@ EXPORTED = (
     "nz_natural_destroy", "nz_natural_pattern", "nz_natural_set_history",
     "nz_update_state", "nz_residual", "nz_jacobian", "nz_diag_fma_peak",
     "nz_flash_batch_noalloc", "nz_natural_init_ptz", "nz_natural_set_update_mode",
-    "nz_flash_check", "nz_ctx_set_spin_limit",
+    "nz_flash_check", "nz_ctx_set_spin_limit", "nz_jacobian_columns",
 )
 
 _lib = None
@@ -60,6 +60,7 @@ def load():
         L.nz_natural_set_update_mode.argtypes = [vp, i32]
         L.nz_residual.argtypes = [vp, vp, vp, vp, vp]
         L.nz_jacobian.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.nz_jacobian_columns.argtypes = [vp, vp, vp, vp, vp, vp]
     L.nz_diag_fma_peak.argtypes = [i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.nz_flash_batch_noalloc.argtypes = [vp, i64, vp, vp, vp, vp, vp, i32, vp]
     L.nz_flash_check.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]

@@ -138,3 +138,17 @@ class NaturalAssembler:
         if rc != 0:
             raise FloatingPointError("Natural Jacobian: domain error")
         return vals
+
+    def assemble_jacobian_columns(self, primary, phase_state, values=None, residual=None, stream=None):
+        """The same values [nnzb, B, B] in cell-column order: cell c's self block
+        and then the block of each of its connections, starting at block
+        c + conn_offset[c] (the values of the reference's per-cell
+        MatSetValuesBlocked column insertion, jacobian.inc:279-299)."""
+        p, s = self._state(primary, phase_state)
+        vals = values if values is not None else torch.empty(self.nnzb, self.B, self.B, dtype=torch.float64,
+                                                             device=self.device)
+        rc = check(self.lib.nz_jacobian_columns(self.handle, _ptr(p), _ptr(s), _ptr(vals), _ptr(residual),
+                                                _stream_ptr(stream)), "nz_jacobian_columns")
+        if rc != 0:
+            raise FloatingPointError("Natural Jacobian: domain error")
+        return vals
