@@ -132,24 +132,25 @@ def cpu_reference_rate(fluid, P, T, z, seconds_target: float = 15.0):
             "single_core_us_per_flash": per_point * 1e6}
 
 
-def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: bool):
+def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: bool, with_cpa: bool = True):
     """One Natural Newton evaluation (transactional phase-state update of a
-    perturbed iterate + residual + BAIJ Jacobian) on two grids:
+    perturbed iterate + residual + BAIJ Jacobian) on three grids:
 
-    * the 60x20x1 H2O/CO2/nC10 case (1200 cells, 2320 faces), beside the
-      reference's own loops on one host core (the reference runtime is one
-      thread per MPI rank);
-    * a 200x200x50 grid (2,000,000 cells, 5.94 M faces) of the same fluid, for
-      the Jacobian's HBM roofline (its values are written once, 100 doubles per
-      block: algorithmic bytes = blocks x B^2 x 8 + residual).
+    * the 60x20x1 H2O/CO2/nC10 case (1200 cells, 2320 faces), PR, beside the
+      reference's own loops on one host core and on all host cores;
+    * a 200x200x50 grid (2,000,000 cells, 5.94 M faces) of the same fluid;
+    * the 200x200x50 benchmark grid with the six-component PR-CPA fluid
+      (hydrostatic P, B = 19), the Jacobian's HBM roofline and the device to
+      host copy of its BAIJ values (what a host PETSc insertion needs).
+    Jacobian roofline: algorithmic bytes = blocks x B^2 x 8 + residual, written
+    once per evaluation.
     """
     import torch
     from nonenone_b200 import abi, synth
     from nonenone_b200.flash import CubicThreePhaseFlash, Context
-    from nonenone_b200.fluids import make_fluid
+    from nonenone_b200.fluids import make_cpa_six, make_fluid
     from nonenone_b200.natural import NaturalAssembler
     relperm = abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10)
-    fluid = make_fluid()
     results = {}
 
     def events():
@@ -163,21 +164,36 @@ def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: boo
         torch.cuda.synchronize()
         return a.elapsed_time(b)
 
-    for label, shape in (("60x20x1", (60, 20, 1)), ("200x200x50", (200, 200, 50))):
-        grid, P, z = synth.natural_case(0, nx=shape[0], ny=shape[1], nz=shape[2])
+    cases = [("60x20x1", "pr3", (60, 20, 1)), ("200x200x50", "pr3", (200, 200, 50))]
+    if with_cpa:
+        cases.append(("200x200x50_nc6_cpa", "cpa6", (200, 200, 50)))
+    for label, fluid_name, shape in cases:
+        t_setup = time.perf_counter()
+        if fluid_name == "cpa6":
+            grid, P, z, depth = synth.natural_case_hydrostatic(3, nx=shape[0], ny=shape[1], nz=shape[2])
+            fluid = make_cpa_six()
+            temperature = 373.15 + 0.03 * float(np.median(depth))
+            scale = 0.2
+        else:
+            grid, P, z = synth.natural_case(0, nx=shape[0], ny=shape[1], nz=shape[2])
+            fluid = make_fluid()
+            temperature = 353.15
+            scale = 1.0
         ctx = Context(fluid, device=local)
-        nat = NaturalAssembler(ctx, grid, 864.0, 353.15, relperm)
+        nat = NaturalAssembler(ctx, grid, 864.0, temperature, relperm)
         # cells whose P-T-z flash the reference cannot converge (a few per
         # million) take a converged cell's inputs, so the initial state exists
         fl = CubicThreePhaseFlash(fluid, device=local)
-        st = fl.flash(P, np.full(grid.ncell, 353.15), np.ascontiguousarray(z.T),
+        st = fl.flash(P, np.full(grid.ncell, temperature), np.ascontiguousarray(z.T),
                       precision=abi.PRECISION_FP64_STAGED)["status"].cpu().numpy()
         bad, good = np.where(st != 0)[0], np.where(st == 0)[0]
         P, z = P.copy(), z.copy()
         P[bad], z[bad] = P[good[:bad.size]], z[good[:bad.size]]
         primary, ps = nat.initialize_from_ptz(P, z)
         nat.refresh_history(primary, ps)
-        cur_np = synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), NC, 11, 1.0)
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t_setup
+        cur_np = synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), fluid.nc, 11, scale)
         cur = torch.as_tensor(cur_np, device=primary.device)
         F = torch.empty_like(cur)
         vals = torch.empty(nat.nnzb, nat.B, nat.B, dtype=torch.float64, device=primary.device)
@@ -200,22 +216,32 @@ def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: boo
         t_res = sorted(timed(lambda: nat.form_function(cur, ps, out=F)) for _ in range(max(n_rep, 3)))
         t_jac = sorted(timed(lambda: nat.assemble_jacobian(cur, ps, values=vals)) for _ in range(max(n_rep, 3)))
         t_newton = sorted(timed(newton) for _ in range(n_rep))
-        # the same update with every stability test inside the per-cell code
+        # both update forms: every stability test and reflash on the batched
+        # staged kernels, or inside each cell's own thread / warp
+        nat.set_update_mode("staged")
+        t_update_staged = sorted(timed(update) for _ in range(n_rep))
         nat.set_update_mode("per_cell")
         t_update_per_cell = timed(update)
         nat.set_update_mode("auto")
         rc, rep = update()
         jac_bytes = nat.nnzb * nat.B * nat.B * 8 + grid.ncell * nat.B * 8
         jac_ms = t_jac[len(t_jac) // 2]
+        host_vals = torch.empty(vals.shape, dtype=vals.dtype, pin_memory=True)
+        d2h_ms = timed(lambda: host_vals.copy_(vals, non_blocking=True))
         entry = {
             "cells": grid.ncell, "faces": int(grid.nfaces), "block": nat.B, "blocks": nat.nnzb,
+            "fluid": "six-component PR-CPA (4C water, CO2 acceptor)" if fluid_name == "cpa6"
+                     else "H2O/CO2/nC10 PR", "temperature_K": temperature,
+            "setup_s": setup_s,
             "newton_eval_ms": {"p50": t_newton[len(t_newton) // 2], "max": t_newton[-1], "reps": n_rep},
             "cell_evals_per_s": grid.ncell / (t_newton[len(t_newton) // 2] * 1e-3),
             "update_ms": t_update[len(t_update) // 2],
-            "update_form": "staged" if grid.ncell >= 148 * 256 else "per-cell (warp per cell)",
+            "update_form_auto": "staged" if grid.ncell >= 148 * 256 else "per-cell (warp per cell)",
+            "update_ms_staged_form": t_update_staged[len(t_update_staged) // 2],
             "update_ms_per_cell_form": t_update_per_cell,
             "residual_ms": t_res[len(t_res) // 2],
             "jacobian_ms": jac_ms,
+            "baij_device_to_host_ms": d2h_ms,
             "update_committed": rc == 0,
             "stable_reduced_cells": int(rep.stable_reduced_cells),
             "jacobian_roofline": {"bound": "hbm", "bytes_per_launch": jac_bytes,
@@ -227,22 +253,25 @@ def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: boo
             try:
                 from oracle import ref
                 if ref.available():
-                    oracle = ref.Natural(fluid, grid, 864.0, 353.15, relperm)
+                    cpu = {}
                     p0, s0 = primary.cpu().numpy(), ps.cpu().numpy()
-                    oracle.set_history(p0, s0)
-                    t0 = time.perf_counter()
-                    oracle.update_state(cur_np, s0)
-                    oracle.residual(cur_np, s0)
-                    oracle.jacobian(cur_np, s0)
-                    dt = time.perf_counter() - t0
-                    entry["cpu_reference"] = {
-                        "newton_eval_ms": dt * 1e3, "cell_evals_per_s": grid.ncell / dt, "cores": 1,
-                        "kind": "reference", "what": "the reference's updatePhaseState / residual / "
-                                                    "Jacobian loops (oracle/_ref), one thread, same state"}
+                    for threads in (1, os.cpu_count() or 1):
+                        oracle = ref.Natural(fluid, grid, 864.0, temperature, relperm)
+                        oracle.set_threads(threads)
+                        oracle.set_history(p0, s0)
+                        t0 = time.perf_counter()
+                        oracle.update_state(cur_np, s0)
+                        oracle.residual(cur_np, s0)
+                        oracle.jacobian(cur_np, s0)
+                        dt = time.perf_counter() - t0
+                        cpu[f"{threads}_threads"] = {"newton_eval_ms": dt * 1e3, "cell_evals_per_s": grid.ncell / dt}
+                    entry["cpu_reference"] = {**cpu, "kind": "reference",
+                                              "what": "the reference's updatePhaseState / residual / Jacobian "
+                                                      "loops (oracle/_ref) on the same state, one kernel per thread"}
             except Exception as ex:
                 entry["cpu_reference"] = {"error": str(ex)}
         results[label] = entry
-        del nat, ctx, fl, vals
+        del nat, ctx, fl, vals, host_vals
         torch.cuda.empty_cache()
     return results
 
@@ -554,7 +583,7 @@ def run_gpu(args):
                 hbm_peak = float(json.load(fh)["hbm_gbs"])
         except Exception:
             hbm_peak = 6650.0
-        natural = natural_measure(local, 5, hbm_peak, not args.no_cpu_baseline)
+        natural = natural_measure(local, 5, hbm_peak, not args.no_cpu_baseline, not args.no_cpa_natural)
 
     if rank == 0:
         cpu = None
@@ -633,6 +662,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-natural", action="store_true",
                     help="skip the Natural Newton-evaluation measurements")
+    ap.add_argument("--no-cpa-natural", action="store_true",
+                    help="skip the six-component PR-CPA Natural grid")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

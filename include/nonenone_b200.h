@@ -103,8 +103,8 @@ typedef struct nz_fluid_desc {
      * The flash and EOS entry points carry one associating component with equal
      * donor and acceptor sites, or one donor-bearing component with any acceptors
      * (e.g. 4C water with CO2 as an acceptor); fluids with several donor-bearing
-     * components give NZ_FLASH_NOT_PORTED per point.  The Natural entry points
-     * refuse CPA. */
+     * components give NZ_FLASH_NOT_PORTED per point, and nz_natural_create
+     * refuses them. */
     double cpa_a0[NZ_MAX_NC];            /* Pa m6/mol2 */
     double cpa_b[NZ_MAX_NC];             /* m3/mol */
     double cpa_c1[NZ_MAX_NC];

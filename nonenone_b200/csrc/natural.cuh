@@ -16,6 +16,7 @@
 #pragma once
 
 #include "dual.cuh"
+#include "cpa.cuh"
 
 namespace nz
 {
@@ -372,7 +373,8 @@ NZ_HD bool cellProperties(const FluidDev &F, const NatConst &K, const CellStateT
     }
     const S T = S(K.temperature);
     S A[NC][NC], Bi[NC];
-    mixingT<NC, S>(F, st.p, T, false, A, Bi);
+    if (F.eosModel != EOS_CPA)
+        mixingT<NC, S>(F, st.p, T, false, A, Bi);
     for (int ph = 0; ph < 3; ++ph)
     {
         pr.saturation[ph] = st.sat[ph];
@@ -382,12 +384,25 @@ NZ_HD bool cellProperties(const FluidDev &F, const NatConst &K, const CellStateT
             mixingT<NC, S>(F, st.p, T, true, Aw, Bw);
         const S(&Ap)[NC][NC] = aq ? Aw : A;
         const S(&Bp)[NC] = aq ? Bw : Bi;
-        S Si[NC], Am, Bm;
-        phaseMixT<NC, S>(comp[ph], Ap, Bp, Si, Am, Bm);
-        bool ok = true;
-        const S Z = cubicRootT<S>(Am, Bm, F.m1, F.m2, ph == GAS, ok);
-        if (!ok || !fugacityT<NC, S>(st.p, comp[ph], Bp, Si, Am, Bm, Z, F.m1, F.m2, pr.f[ph]))
-            return false;
+        S Z;
+        if (F.eosModel == EOS_CPA)
+        {
+            // CPA keeps the full phaseResult path per phase (:336-352)
+            S phi[NC];
+            if (cpaPhaseT<NC, S>(F, st.p, K.temperature, comp[ph], ph != GAS, Z, phi) != ERR_NONE)
+                return false;
+            for (int i = 0; i < NC; ++i)
+                pr.f[ph][i] = phi[i] * st.p * comp[ph][i];
+        }
+        else
+        {
+            S Si[NC], Am, Bm;
+            phaseMixT<NC, S>(comp[ph], Ap, Bp, Si, Am, Bm);
+            bool ok = true;
+            Z = cubicRootT<S>(Am, Bm, F.m1, F.m2, ph == GAS, ok);
+            if (!ok || !fugacityT<NC, S>(st.p, comp[ph], Bp, Si, Am, Bm, Z, F.m1, F.m2, pr.f[ph]))
+                return false;
+        }
         // eosFlowProperties (fluid_system.hpp:99-125), no volume translation
         S total = S(0.0);
         for (int i = 0; i < NC; ++i)

@@ -335,8 +335,14 @@ int nz_natural_create(nz_ctx *ctx, const nz_natural_desc *desc, nz_natural **out
     *out = nullptr;
     if (!ctx || !desc)
         return setError(NZ_ERR_ARGUMENT, "nz_natural_create: null argument");
-    if (ctx->fluid.eosModel == nz::EOS_CPA)
-        return setError(NZ_ERR_UNSUPPORTED, "nz_natural_create: the Natural kernels carry PR and SW, not CPA");
+    if (ctx->fluid.eosModel == nz::EOS_CPA && ctx->fluid.cpa.symmetric < 0 && ctx->fluid.cpa.singleDonor < 0)
+    {
+        for (int i = 0; i < ctx->fluid.nc; ++i)
+            if (ctx->fluid.cpa.donor[i] > 0)
+                return setError(NZ_ERR_UNSUPPORTED,
+                                "nz_natural_create: CPA with several donor-bearing components needs the general "
+                                "association solve, which this build does not carry");
+    }
     if (ctx->fluid.water < 0)
         return setError(NZ_ERR_ARGUMENT, "nz_natural_create: the fully compositional model needs a water component");
     const nz_natural_desc &d = *desc;

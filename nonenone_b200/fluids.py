@@ -152,3 +152,22 @@ def make_cpa_h2o_co2_nc10(co2_acceptor: bool = True) -> FluidDesc:
         d.cpa_cross_epsilon[0 * MAX_NC + 1] = 8061.5
         d.cpa_cross_beta[0 * MAX_NC + 1] = 0.15182
     return d
+
+
+def make_cpa_six() -> FluidDesc:
+    """The six-component PR-CPA fluid of the 200x200x50 benchmark grid:
+    {H2O, CO2, C1, nC4, nC10, nC16} with the critical data and BIPs of
+    make_fluid(SIX_COMPONENT), water self-associating with the 4C parameters
+    of make_cpa_h2o_co2_nc10 and CO2 a cross-associating acceptor (the
+    single-donor association path), PR physical term."""
+    names = SIX_COMPONENT
+    d = make_fluid(names, eos_type=5)
+    set_cpa(d, names, CPA_PR, water=dict(a0=0.15782, b=1.4788e-5, c1=0.6736, epsilon=16123.0,
+                                         beta=0.069662, donor=2, acceptor=2))
+    co2 = names.index("CO2")
+    w = names.index("H2O")
+    d.cpa_epsilon[co2], d.cpa_beta[co2] = 8061.5, 0.15182
+    d.cpa_acceptor_sites[co2] = 1
+    d.cpa_cross_epsilon[w * MAX_NC + co2] = 8061.5
+    d.cpa_cross_beta[w * MAX_NC + co2] = 0.15182
+    return d

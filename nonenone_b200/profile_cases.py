@@ -3,7 +3,7 @@
   python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged|mixed]
       one N-point batch of the seeded flash mixture (after a 4,096-point warm-up
       batch, so kernels of the measured batch come second)
-  python -m nonenone_b200.profile_cases natural NX NY NZ [--update] [--per-cell]
+  python -m nonenone_b200.profile_cases natural NX NY NZ [--update] [--per-cell] [--fluid pr3|cpa6]
       P-T-z initialisation of an NX x NY x NZ grid of the H2O/CO2/nC10 case,
       then two residual + Jacobian evaluations of the accepted state; with
       --update first one transactional phase-state update of a perturbed
@@ -39,26 +39,41 @@ def run_flash(n: int, precision: str) -> None:
           f"{fl.eos_eval_count()} EOS evaluations")
 
 
-def run_natural(nx: int, ny: int, nz: int, update: bool = False, per_cell: bool = False) -> None:
+def run_natural(nx: int, ny: int, nz: int, update: bool = False, per_cell: bool = False,
+                fluid_name: str = "pr3", scale: float = 1.0) -> None:
+    import time
+
     import torch
     from . import abi, synth
     from .flash import Context, CubicThreePhaseFlash
-    from .fluids import make_fluid
+    from .fluids import make_cpa_six, make_fluid
     from .natural import NaturalAssembler
-    grid, P, z = synth.natural_case(0, nx=nx, ny=ny, nz=nz)
-    fluid = make_fluid()
+    t_start = time.perf_counter()
+    if fluid_name == "cpa6":
+        grid, P, z, depth = synth.natural_case_hydrostatic(3, nx=nx, ny=ny, nz=nz)
+        fluid = make_cpa_six()
+        temperature = 373.15 + 0.03 * float(np.median(depth))
+    else:
+        grid, P, z = synth.natural_case(0, nx=nx, ny=ny, nz=nz)
+        fluid = make_fluid()
+        temperature = 353.15
     ctx = Context(fluid)
-    nat = NaturalAssembler(ctx, grid, 864.0, 353.15, abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10))
+    nat = NaturalAssembler(ctx, grid, 864.0, temperature, abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10))
     fl = CubicThreePhaseFlash(fluid)
-    st = fl.flash(P, np.full(grid.ncell, 353.15), np.ascontiguousarray(z.T),
+    st = fl.flash(P, np.full(grid.ncell, temperature), np.ascontiguousarray(z.T),
                   precision=abi.PRECISION_FP64_STAGED)["status"].cpu().numpy()
+    print(f"P-T-z flash of {grid.ncell} cells ({fluid_name}): {time.perf_counter() - t_start:.1f} s, "
+          f"{int((st != 0).sum())} not converged")
     bad, good = np.where(st != 0)[0], np.where(st == 0)[0]
     P[bad], z[bad] = P[good[:bad.size]], z[good[:bad.size]]
+    t0 = time.perf_counter()
     primary, ps = nat.initialize_from_ptz(P, z)
+    torch.cuda.synchronize()
+    print(f"initialisation of {grid.ncell} cells: {time.perf_counter() - t0:.1f} s")
     nat.refresh_history(primary, ps)
     if update:
         nat.set_update_mode("per_cell" if per_cell else "staged")
-        cur = torch.as_tensor(synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), fluid.nc, 11, 1.0),
+        cur = torch.as_tensor(synth.perturb_natural_state(primary.cpu().numpy(), ps.cpu().numpy(), fluid.nc, 11, scale),
                               device=primary.device)
         work_s = ps.clone()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -103,11 +118,14 @@ def main(argv=None) -> int:
     nat.add_argument("nz", type=int)
     nat.add_argument("--update", action="store_true")
     nat.add_argument("--per-cell", action="store_true")
+    nat.add_argument("--fluid", default="pr3", choices=["pr3", "cpa6"],
+                     help="pr3: H2O/CO2/nC10 PR; cpa6: the six-component PR-CPA fluid on the hydrostatic grid")
+    nat.add_argument("--scale", type=float, default=1.0, help="perturbation scale of the updated iterate")
     a = ap.parse_args(argv)
     if a.case == "flash":
         run_flash(a.n, a.precision)
     else:
-        run_natural(a.nx, a.ny, a.nz, a.update, a.per_cell)
+        run_natural(a.nx, a.ny, a.nz, a.update, a.per_cell, a.fluid, a.scale)
     return 0
 
 

@@ -158,6 +158,30 @@ def natural_case(seed: int = 0, nx: int = 60, ny: int = 20, nz: int = 1,
     return grid, P, np.ascontiguousarray(z)
 
 
+def natural_case_hydrostatic(seed: int = 3, nx: int = 200, ny: int = 200, nz: int = 50,
+                             dx: float = 10.0, dy: float = 10.0, dz: float = 2.0,
+                             perm_median_md: float = 50.0, perm_sigma_ln: float = 1.5, kv_kh: float = 0.1,
+                             porosity=(0.05, 0.30), p_top: float = 20.0e6, p_gradient: float = 0.01e6,
+                             alpha=(4.0, 2.0, 1.0, 1.0, 1.0, 1.0)):
+    """The 3-D benchmark grid: nx x ny x nz cells of dx x dy x dz m (200 x 200
+    x 50 of 10 x 10 x 2 m: 2,000,000 cells, 5.94 M faces), permeability
+    lognormal (median 50 mD, sigma_ln 1.5, kv/kh 0.1), porosity U[0.05, 0.30],
+    hydrostatic pressure p_top + p_gradient x depth of the cell centre (20 MPa
+    + 0.01 MPa/m), z ~ Dirichlet(alpha).  Returns (grid, P[ncell], z[ncell, nc],
+    depth[ncell])."""
+    from .grid import MILLIDARCY, StructuredGrid, axis_centers
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    kh = perm_median_md * MILLIDARCY * np.exp(perm_sigma_ln * rng.standard_normal(n))
+    perm = np.stack([kh, kh, kh * kv_kh], axis=1)
+    phi = rng.uniform(porosity[0], porosity[1], n)
+    grid = StructuredGrid(nx, ny, nz, dx, dy, dz, perm, phi)
+    depth = axis_centers(np.full(nz, float(dz)))[grid.k]
+    P = p_top + p_gradient * depth
+    z = rng.dirichlet(list(alpha), n)
+    return grid, P, np.ascontiguousarray(z), depth
+
+
 # Quadratic relative permeabilities of the reference's H2O-CO2-nC10 case
 # (case/h2o_co2_nc10_2d_benchmark/benchmark_common.hpp:97-126).
 RELPERM_H2O_CO2_NC10 = dict(swc=0.10, sorw=0.15, sgc=0.02, sorg=0.10,

@@ -49,6 +49,8 @@ def lib():
         L.nzref_residual.argtypes = [vp, vp, vp, vp]
         L.nzref_jacobian.argtypes = [vp, vp, vp, vp]
         L.nzref_natural_pattern.argtypes = [vp, vp, vp, vp]
+        L.nzref_natural_set_threads.argtypes = [vp, i32]
+        L.nzref_natural_set_threads.restype = None
         _lib = L
     return _lib
 
@@ -184,6 +186,11 @@ class Natural:
         if rc != 0:
             raise RuntimeError(f"PTz flash failed at cell {rc - 1}")
         return primary, ps
+
+    def set_threads(self, threads: int):
+        """Worker threads of the cell loops (one kernel each); the results do
+        not depend on the count."""
+        lib().nzref_natural_set_threads(self.h, int(threads))
 
     def set_history(self, primary, ps):
         _check(lib().nzref_natural_set_history(self.h, _p(primary), _p(ps)))

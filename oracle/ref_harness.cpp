@@ -360,6 +360,7 @@ struct NaturalBase
     virtual int initPtz(const double *P, const double *z, double *primary, double *ps) = 0;
     virtual int setHistory(const double *primary, const double *ps) = 0;
     virtual int updateState(double *primary, double *ps, nz_report *report) = 0;
+    virtual void setThreads(int n) = 0;
     virtual int residual(const double *primary, const double *ps, double *F) = 0;
     virtual int jacobian(const double *primary, const double *ps, double *vals) = 0;
     virtual int pattern(int64_t *rowPtr, int64_t *colIdx, int64_t *nnzb) = 0;
@@ -381,6 +382,20 @@ struct Natural final : NaturalBase
 
     std::unique_ptr<FluidSystem<I>> fluid;
     std::unique_ptr<Kernel> kernel;
+    // Worker threads of the cell loops, one kernel each (the flash inside a
+    // kernel keeps a mutable parameter cache, three_phase_flash.hpp:598).
+    int threads{1};
+    std::vector<std::unique_ptr<Kernel>> workers;
+
+    void setThreads(int n) override
+    {
+        threads = n < 1 ? 1 : n;
+        workers.resize(static_cast<std::size_t>(threads));
+        for (int t = 1; t < threads; ++t)
+            if (!workers[t])
+                workers[t] = std::make_unique<Kernel>(*fluid);
+    }
+    const Kernel &worker(int t) const { return t == 0 ? *kernel : *workers[static_cast<std::size_t>(t)]; }
     int64_t ncell{0};
     std::vector<double> porosity, volume, trans, grav;
     std::vector<int64_t> offset, neighbor;
@@ -537,17 +552,19 @@ struct Natural final : NaturalBase
     {
         // buildCellCache_ (natural_petsc_runtime_cell_cache.inc:66-116)
         std::vector<CacheEntry> cache(static_cast<std::size_t>(ncell));
-        for (int64_t c = 0; c < ncell; ++c)
-        {
-            const auto a = readPrimary(primary, c);
-            const auto s = readPs(ps, c);
-            cache[c].state = kernel->decodeState(a, s);
-            typename Kernel::Composition overall{};
-            for (int i = 0; i < NC; ++i)
-                overall[i] = Eval(s.overallComposition[i]);
-            cache[c].props = kernel->evaluateProperties(
-                cache[c].state, Eval(porosity[c]), 0.0, 2.0, &overall);
-        }
+        parallelFor(ncell, threads, [&](int64_t b, int64_t e, int t) {
+            const Kernel &k = worker(t);
+            for (int64_t c = b; c < e; ++c)
+            {
+                const auto a = readPrimary(primary, c);
+                const auto s = readPs(ps, c);
+                cache[c].state = k.decodeState(a, s);
+                typename Kernel::Composition overall{};
+                for (int i = 0; i < NC; ++i)
+                    overall[i] = Eval(s.overallComposition[i]);
+                cache[c].props = k.evaluateProperties(cache[c].state, Eval(porosity[c]), 0.0, 2.0, &overall);
+            }
+        });
         return cache;
     }
 
@@ -579,22 +596,32 @@ struct Natural final : NaturalBase
         nz_report r{};
         r.succeeded = 1;
         r.first_failure_cell = -1;
-        const auto &eq = kernel->phaseEquilibrium();
+        // every cell's update (independent), then the transaction in cell order
+        std::vector<PhaseUpdateResult> results(static_cast<std::size_t>(ncell));
+        parallelFor(ncell, threads, [&](int64_t b, int64_t e, int t) {
+            const auto &eq = worker(t).phaseEquilibrium();
+            for (int64_t c = b; c < e; ++c)
+            {
+                auto a = readPrimary(primary, c);
+                auto s = readPs(ps, c);
+                eq.sanitizePrimaryBeforeFlash(a, false);
+                PhaseUpdateResult u;
+                try
+                {
+                    u = eq.updatePhaseState(a, s);
+                }
+                catch (const std::exception &)
+                {
+                    u.status = PhaseUpdateStatus::RecoverableThermodynamicFailure;
+                }
+                results[c] = u;
+                newPrimary[c] = a;
+                newPs[c] = s;
+            }
+        });
         for (int64_t c = 0; c < ncell; ++c)
         {
-            auto a = readPrimary(primary, c);
-            auto s = readPs(ps, c);
-            eq.sanitizePrimaryBeforeFlash(a, false);
-            PhaseUpdateResult u;
-            try
-            {
-                u = eq.updatePhaseState(a, s);
-            }
-            catch (const std::exception &ex)
-            {
-                g_error = ex.what();
-                u.status = PhaseUpdateStatus::RecoverableThermodynamicFailure;
-            }
+            const PhaseUpdateResult &u = results[c];
             if (u.recoverableFailure())
             {
                 r.succeeded = 0;
@@ -611,8 +638,6 @@ struct Natural final : NaturalBase
             ++r.updated_cells;
             if (u.status == PhaseUpdateStatus::StableReducedSet)
                 ++r.stable_reduced_cells;
-            newPrimary[c] = a;
-            newPs[c] = s;
         }
         if (report) *report = r;
         if (!r.succeeded)
@@ -630,7 +655,9 @@ struct Natural final : NaturalBase
         if (previousAccumulation.size() != static_cast<std::size_t>(ncell))
             return -1;
         const auto cache = buildCache(primary, ps);
-        for (int64_t c = 0; c < ncell; ++c)
+        parallelFor(ncell, threads, [&](int64_t b, int64_t e, int t) {
+        const Kernel &k = worker(t);
+        for (int64_t c = b; c < e; ++c)
         {
             FaceMassFlux<I, double> outward{};
             for (int64_t k = offset[c]; k < offset[c + 1]; ++k)
@@ -642,14 +669,15 @@ struct Natural final : NaturalBase
                 for (int i = 0; i < NC; ++i)
                     outward.component[i] += flux.component[i];
             }
-            auto block = kernel->assembleLocalResidual(
+            auto block = k.assembleLocalResidual(
                 cache[c].state, cache[c].props, previousProperties[c], volume[c], dt,
                 fscale, -1, 2650.0, nullptr, &previousAccumulation[c], nullptr);
             std::array<Eval, NC> zeroSource{};
             addCellConservationTransportAndWell<I>(block, outward, zeroSource, Eval(0.0));
-            for (int k = 0; k < B; ++k)
-                F[c * B + k] = block.value[k].value();
+            for (int q = 0; q < B; ++q)
+                F[c * B + q] = block.value[q].value();
         }
+        });
         return 0;
     }
 
@@ -659,9 +687,11 @@ struct Natural final : NaturalBase
             return -1;
         const auto cache = buildCache(primary, ps);
         std::fill(vals, vals + rowPtr.back() * B * B, 0.0);
-        for (int64_t c = 0; c < ncell; ++c)
+        parallelFor(ncell, threads, [&](int64_t b, int64_t e, int t) {
+        const Kernel &k = worker(t);
+        for (int64_t c = b; c < e; ++c)
         {
-            const auto block = kernel->assembleLocalResidual(
+            const auto block = k.assembleLocalResidual(
                 cache[c].state, cache[c].props, previousProperties[c], volume[c], dt,
                 fscale, -1, 2650.0, nullptr, &previousAccumulation[c], nullptr);
             double *self = vals + selfSlot[c] * B * B;
@@ -687,6 +717,7 @@ struct Natural final : NaturalBase
                 }
             }
         }
+        });
         return 0;
     }
 };
@@ -934,6 +965,10 @@ int nzref_residual(void *h, const double *primary, const double *ps, double *F)
 int nzref_jacobian(void *h, const double *primary, const double *ps, double *vals)
 {
     return guarded([&] { return static_cast<NaturalBase *>(h)->jacobian(primary, ps, vals); });
+}
+void nzref_natural_set_threads(void *h, int threads)
+{
+    static_cast<NaturalBase *>(h)->setThreads(threads);
 }
 int nzref_natural_pattern(void *h, int64_t *rowPtr, int64_t *colIdx, int64_t *nnzb)
 {

@@ -112,7 +112,7 @@ double compare(const Bcsr &m, const std::vector<double> &ref, int64_t ncell, int
                     const size_t e = (size_t(s) * B + r) * B + k;
                     const double a = m.values[e], b = ref[e];
                     const double floor = 1.0e-6 * scale;
-                    if (std::fabs(b) < floor)
+                    if (b != 0.0 && std::fabs(b) < floor)
                         ++*floored;
                     const double denom = std::max(std::fabs(b), floor);
                     const double err = denom > 0.0 ? std::fabs(a - b) / denom : std::fabs(a - b);
@@ -225,7 +225,7 @@ int main(int argc, char **argv)
     const double errColumns = compare(a, reference, ncell, B, &floored);
     const double errRows = compare(rowwise, reference, ncell, B, &floored);
     std::printf("cells %lld blocks %lld B %d: column insertion max err %.3e, block insertion max err %.3e, "
-                "entries under the row floor %lld of %zu\n",
+                "nonzero entries under the row floor %lld of %zu\n",
                 (long long)ncell, (long long)nnzb, B, errColumns, errRows, (long long)floored,
                 a.values.size());
     cudaFree(dHist);

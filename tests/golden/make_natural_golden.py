@@ -9,6 +9,8 @@ of the runtime loops, calling the reference's kernels); inputs are seeded
   natural_pr_nc3.npz  12x6x2 grid (gravity faces), H2O/CO2/nC10, PR
   natural_sw_nc3.npz  6x4x2 grid, Soreide-Whitson, salinity 1 mol/kg
   natural_pr_nc6.npz  6x4x1 grid, six components, PR
+  natural_cpa_nc3.npz 6x4x2 grid, PR-CPA H2O/CO2/nC10 (4C water, CO2 acceptor)
+  natural_cpa_nc6.npz 4x3x2 grid, six components, PR-CPA (4C water, CO2 acceptor)
 
 Each holds the grid arrays, the P-T-z initial state (primary, phase_state), the
 history accumulation, a perturbed Newton iterate (``current``) with its residual,
@@ -27,7 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from nonenone_b200 import abi, synth  # noqa: E402
-from nonenone_b200.fluids import SIX_COMPONENT, make_fluid  # noqa: E402
+from nonenone_b200.fluids import SIX_COMPONENT, make_cpa_h2o_co2_nc10, make_cpa_six, make_fluid  # noqa: E402
 from oracle import ref  # noqa: E402
 
 TIME_STEP = 864.0
@@ -90,6 +92,8 @@ def main():
     make("natural_pr_nc3.npz", make_fluid(), 0, (12, 6, 2), (2.0, 1.0, 1.0))
     make("natural_sw_nc3.npz", make_fluid(eos_model=abi.EOS_SW, salinity=1.0), 4, (6, 4, 2), (2.0, 1.0, 1.0))
     make("natural_pr_nc6.npz", make_fluid(SIX_COMPONENT), 5, (6, 4, 1), (4.0, 2.0, 1.0, 1.0, 1.0, 1.0))
+    make("natural_cpa_nc3.npz", make_cpa_h2o_co2_nc10(), 6, (6, 4, 2), (2.0, 1.0, 1.0), scale=0.2)
+    make("natural_cpa_nc6.npz", make_cpa_six(), 7, (4, 3, 2), (4.0, 2.0, 1.0, 1.0, 1.0, 1.0), scale=0.2)
 
 
 if __name__ == "__main__":

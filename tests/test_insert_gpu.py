@@ -63,12 +63,16 @@ def test_insert_program_builds(tmp_path):
 @pytest.mark.parametrize("fixture,fluid_args", [
     ("natural_pr_nc3.npz", dict()),
     ("natural_pr_nc6.npz", dict(six=True)),
+    ("natural_cpa_nc6.npz", dict(cpa6=True)),
 ])
 def test_cpp_host_inserts_the_jacobian_like_petsc(tmp_path, fixture, fluid_args):
     from nonenone_b200 import abi, synth
-    from nonenone_b200.fluids import SIX_COMPONENT, make_fluid
+    from nonenone_b200.fluids import SIX_COMPONENT, make_cpa_six, make_fluid
     exe = _build(tmp_path)
-    fluid = make_fluid(SIX_COMPONENT) if fluid_args.get("six") else make_fluid()
+    if fluid_args.get("cpa6"):
+        fluid = make_cpa_six()
+    else:
+        fluid = make_fluid(SIX_COMPONENT) if fluid_args.get("six") else make_fluid()
     relperm = abi.RelpermDesc(**synth.RELPERM_H2O_CO2_NC10)
     case = str(tmp_path / "case")
     _write_case(case, fixture, fluid, relperm)

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from nonenone_b200 import abi, synth
-from nonenone_b200.fluids import SIX_COMPONENT, make_fluid
+from nonenone_b200.fluids import SIX_COMPONENT, make_cpa_h2o_co2_nc10, make_cpa_six, make_fluid
 
 pytestmark = pytest.mark.gpu
 
@@ -28,6 +28,8 @@ CASES = {
     "natural_pr_nc3.npz": lambda: make_fluid(),
     "natural_sw_nc3.npz": lambda: make_fluid(eos_model=abi.EOS_SW, salinity=1.0),
     "natural_pr_nc6.npz": lambda: make_fluid(SIX_COMPONENT),
+    "natural_cpa_nc3.npz": lambda: make_cpa_h2o_co2_nc10(),
+    "natural_cpa_nc6.npz": lambda: make_cpa_six(),
 }
 
 
@@ -73,6 +75,12 @@ def assert_entries(gpu, ref, axis_eq, what):
     with np.errstate(invalid="ignore"):
         err = np.where(fin, np.abs(gpu - ref) / np.where(denom > 0, denom, 1.0), 0.0)
     worst = np.unravel_index(np.argmax(err), err.shape)
+    under = fin & (ref != 0) & (np.abs(ref) < FLOOR * scale)
+    rel = np.where(fin & (ref != 0), np.abs(gpu - ref) / np.where(ref != 0, np.abs(ref), 1.0), 0.0)
+    print(f"[entries] {what}: {int(fin.sum())} entries, max err {err.max():.3e}; "
+          f"{int(under.sum())} nonzero entries under the row floor "
+          f"(their largest plain relative error {float(rel[under].max()) if under.any() else 0.0:.3e}); "
+          f"largest plain relative error above the floor {float(rel[fin & ~under].max()):.3e}")
     assert err.max() <= ENTRY_TOL, f"{what}: max err {err.max():.3e} at {worst}: {gpu[worst]} vs {ref[worst]}"
     return err.max()
 
