@@ -221,7 +221,7 @@ struct Equilibrium
         }
     }
 
-    // updateSecondary for PR / SW (:164-280)
+    // updateSecondary (:164-280)
     NZ_HD void updateSecondary(double *primary, PhaseRec<NC> &ps)
     {
         double c[3][NC];
@@ -236,10 +236,29 @@ struct Equilibrium
         {
             if (!(ps.presence & bitOf(ph)))
                 continue;
-            const MixParams<NC> &mp = (ph == WATER && s.sw()) ? s.aq : s.nonAq;
-            PhaseMix<NC> m;
-            phaseMixing<NC>(c[ph], mp, m);
-            const double z = selectCubicRoot(m.A, m.B, s.F->m1, s.F->m2, ph == GAS);
+            double z;
+            if (s.F->eosModel == EOS_CPA)
+            {
+                // eos.compressibility's CPA branch: Z = p / (rho R T) at the
+                // density root (cubic_eos.hpp:865-884)
+                CpaMix<NC> cm;
+                cpaMixing<NC>(*s.F, T, c[ph], cm);
+                double rho = 0.0;
+                const int rc = cpaDensityRoot<NC>(*s.F, p, T, c[ph], ph != GAS, cm, rho);
+                if (rc != ERR_NONE)
+                {
+                    s.fail(rc);
+                    return;
+                }
+                z = p / (rho * kGasConstant * T);
+            }
+            else
+            {
+                const MixParams<NC> &mp = (ph == WATER && s.sw()) ? s.aq : s.nonAq;
+                PhaseMix<NC> m;
+                phaseMixing<NC>(c[ph], mp, m);
+                z = selectCubicRoot(m.A, m.B, s.F->m1, s.F->m2, ph == GAS);
+            }
             if (!isfinite(z))
             {
                 s.fail(ERR_EOS);

@@ -154,13 +154,42 @@ def make_cpa_h2o_co2_nc10(co2_acceptor: bool = True) -> FluidDesc:
     return d
 
 
+# Component sets of the multi-model and serving workloads, by component count:
+# the six-component benchmark set, reduced or extended with C2 / C3.
+MODEL_COMPONENTS = {
+    3: H2O_CO2_NC10,
+    4: ("H2O", "CO2", "C1", "nC10"),
+    5: ("H2O", "CO2", "C1", "nC4", "nC10"),
+    6: SIX_COMPONENT,
+    8: ("H2O", "CO2", "C1", "C2", "C3", "nC4", "nC10", "nC16"),
+}
+
+
+def model_fluid(nc: int, eos: str) -> FluidDesc:
+    """The fluid of one model of the multi-model / serving workloads: the
+    MODEL_COMPONENTS set of `nc` with eos "pr", "sw" (salinity 1 mol/kg) or
+    "cpa" (PR-CPA, 4C water with CO2 as a cross-associating acceptor)."""
+    names = MODEL_COMPONENTS[nc]
+    if eos == "pr":
+        return make_fluid(names)
+    if eos == "sw":
+        return make_fluid(names, eos_model=EOS_SW, salinity=1.0)
+    if eos == "cpa":
+        return make_cpa_names(names)
+    raise ValueError(f"unknown eos {eos!r}")
+
+
 def make_cpa_six() -> FluidDesc:
     """The six-component PR-CPA fluid of the 200x200x50 benchmark grid:
     {H2O, CO2, C1, nC4, nC10, nC16} with the critical data and BIPs of
     make_fluid(SIX_COMPONENT), water self-associating with the 4C parameters
     of make_cpa_h2o_co2_nc10 and CO2 a cross-associating acceptor (the
     single-donor association path), PR physical term."""
-    names = SIX_COMPONENT
+    return make_cpa_names(SIX_COMPONENT)
+
+
+def make_cpa_names(names) -> FluidDesc:
+    """PR-CPA on a component set holding H2O and CO2 (see make_cpa_six)."""
     d = make_fluid(names, eos_type=5)
     set_cpa(d, names, CPA_PR, water=dict(a0=0.15782, b=1.4788e-5, c1=0.6736, epsilon=16123.0,
                                          beta=0.069662, donor=2, acceptor=2))
