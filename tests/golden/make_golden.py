@@ -14,6 +14,10 @@ reference's own FP64 C++ (oracle/_ref/libnzref.so); the inputs are seeded
                     (synth.boundary_points with the reference's own labels): the
                     benchmark's near-boundary slice
   flash_boundary_sw_nc3.npz  256 such points, Soreide-Whitson, salinity ~ U[0,2]
+  bench_boundary_pr_nc3.npz  the benchmark batch's near-boundary slice: 52,429
+                    points (5 % of 1,048,576) of synth.boundary_points with the
+                    reference's labels, inputs only; bench.py's GPU and reference
+                    arms both take it (with the seeded label mixture)
   flash_continuation_pr_nc3.npz  192 points of the 1,048,576-point bench batch
                     (synth.flash_points(2**20, seed=1)) that reach the flash's last
                     fallback, the pressure continuation: 160 it rescues and 32 it
@@ -98,12 +102,15 @@ def main():
     make("flash_pr_nc6.npz", six, P, T, z)
     P, T, z = synth.flash_points(1024, seed=104)
     make("flash_cpa_nc3.npz", make_cpa_h2o_co2_nc10(), P, T, z)
-    labels = lambda P, T, z, s, f=pr: ref.flash_batch(f, P, T, z, salinity=s, threads=8)["presence"]
-    P, T, z = synth.boundary_points(512, labels, seed=105)
+    labels_pr = lambda P, T, z, s, f=pr: ref.flash_batch(f, P, T, z, salinity=s, threads=8)["presence"]
+    P, T, z = synth.boundary_points(512, labels_pr, seed=105)
     make("flash_boundary_pr_nc3.npz", pr, P, T, z)
     labels = lambda P, T, z, s, f=sw: ref.flash_batch(f, P, T, z, salinity=s, threads=8)["presence"]
     P, T, z, s = synth.boundary_points(256, labels, seed=106, salinity=True)
     make("flash_boundary_sw_nc3.npz", sw, P, T, z, s)
+    nb = int(round(synth.BOUNDARY_FRACTION * (1 << 20)))
+    P, T, z = synth.boundary_points(nb, labels_pr, seed=7919)
+    np.savez_compressed(os.path.join(HERE, "bench_boundary_pr_nc3.npz"), P=P, T=T, z=z)
     P, T, z = synth.flash_points(1 << 20, seed=1)
     sel = np.array(RESCUED + FAILING)
     make("flash_continuation_pr_nc3.npz", pr, P[sel], T[sel], np.ascontiguousarray(z[:, sel]))
