@@ -434,11 +434,11 @@ FORMS = ("fp64", "fp64_staged", "mixed")
 def staged_launches(precision_name: str) -> int:
     """Kernels one batch launches: the plain FP64 form one; the staged forms
     start, 8 rounds x 8, recovery 1 (5), recovery 2 (3 x 2), the full solver,
-    2 continuation-anchor launches, select and check (+ the polish of the
+    8 continuation-anchor launches, select and check (+ the polish of the
     mixed form)."""
     if precision_name == "fp64":
         return 1
-    return 1 + 8 * 8 + 5 + 3 * 2 + 1 + 2 + 1 + 1 + (1 if precision_name == "mixed" else 0)
+    return 1 + 8 * 8 + 5 + 3 * 2 + 1 + 8 + 1 + 1 + (1 if precision_name == "mixed" else 0)
 
 
 def form_error(out, ref_out):

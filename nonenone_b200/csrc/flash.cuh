@@ -3726,7 +3726,8 @@ struct Solver
         q.Z[second] = base.result.Z[second];
         if (presenceFromFractions(q.beta) != r.presence)
             return false;
-        deriveReferenceK(q);
+        // the K-values stay the answer's (a move of at most maxChange leaves
+        // them consistent; SW answers do not define them from x alone)
         updateSaturations(P, T, q);
         if (err)
             return false;
@@ -3821,7 +3822,8 @@ struct Solver
         }
         if (presenceFromFractions(q.beta) != r.presence)
             return false;
-        deriveReferenceK(q);
+        // the K-values stay the answer's (a move of at most maxChange leaves
+        // them consistent; SW answers do not define them from x alone)
         updateSaturations(P, T, q);
         if (err)
             return false;

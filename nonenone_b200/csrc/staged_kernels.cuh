@@ -990,8 +990,7 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
 
 // Pressure-continuation anchors of the queued points: one warp per (point,
 // anchor), the lanes splitting the stability seeds as in the recovery kernel.
-// Launched twice: anchor 0 for every queued point (most are decided there),
-// then anchors 1..7 side by side for the points anchor 0 left undecided.
+// Launched once per anchor, for the points the earlier anchors left undecided.
 template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
 stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int first,
@@ -1010,8 +1009,11 @@ stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
     {
         const int64_t k = t / span;
         const int an = first + int(t % span);
-        if (first > 0 && anchors[k * kAnchors].outcome != CONT_NONE)
-            continue;   // decided by anchor 0
+        bool decided = false;
+        for (int earlier = 0; earlier < first; ++earlier)
+            decided = decided || anchors[k * kAnchors + earlier].outcome != CONT_NONE;
+        if (decided)
+            continue;   // an earlier anchor has an outcome: it decides the point
         const int64_t i = a.cont[k];
         if (i < 0 || i >= a.n)
         {
@@ -1113,7 +1115,7 @@ stagedSelectKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
 // (Solver::polish) of every converged multiphase point, read back from and
 // written to the output record (it needs at least the presence, status,
 // fraction, composition and compressibility arrays; fields the caller left
-// out stay out).
+// out stay out; the K-values are the flash's).
 constexpr double kPolishTarget = 1.0e-11;   // largest ln-fugacity residual the polish aims for
 constexpr int kPolishSteps = 4;
 
@@ -1164,11 +1166,6 @@ stagedPolishKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
                 out.composition[(p * NC + c) * a.n + i] = r.x[p][c];
             if (out.compressibility) out.compressibility[p * a.n + i] = r.Z[p];
             if (out.molar_density) out.molar_density[p * a.n + i] = r.rho[p];
-        }
-        for (int c = 0; c < NC; ++c)
-        {
-            if (out.k_gas_oil) out.k_gas_oil[c * a.n + i] = r.Kg[c];
-            if (out.k_water_oil) out.k_water_oil[c * a.n + i] = r.Kw[c];
         }
     }
     warpAddEvals(a.evalCounter, evals);
@@ -1299,8 +1296,11 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     stagedFullKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, out);
     if (after("full", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the full solver");
-    stagedAnchorKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, 0, 1);
-    stagedAnchorKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, 1, kAnchors - 1);
+    // one launch per anchor, each for the points no earlier anchor decided:
+    // the work is the fallback's own (it stops at the first anchor with an
+    // outcome), the points run side by side
+    for (int an = 0; an < kAnchors; ++an)
+        stagedAnchorKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, an, 1);
     stagedSelectKernel<NC><<<unsigned(smCount * 2), kFlashBlock, 0, st>>>(F, a, out);
     if (after("continuation", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the pressure continuation");
