@@ -306,6 +306,88 @@ def serving_measure(local: int, n_requests: int, rate: float = 20.0):
     return stats
 
 
+def models_measure(local: int, nmodels: int, cells, seed: int = 21, precision: int | None = None):
+    """The uneven multi-model batch: `nmodels` models, cell counts log-uniform
+    on `cells`, nc uniform over {3,4,5,6,8}, EOS uniform over PR / SW / PR-CPA,
+    P/T/z drawn as on the hydrostatic benchmark grid (synth.model_points).
+    One ModelBatch (per-nc groups, per-point fluids, one captured CUDA graph,
+    launch shapes from its autotuner) against the same models flashed by
+    separate per-model calls back to back on one stream; both device-event
+    timed, answers compared label for label."""
+    import torch
+    from nonenone_b200 import abi, synth
+    from nonenone_b200.flash import CubicThreePhaseFlash
+    from nonenone_b200.fluids import model_fluid
+    from nonenone_b200.models import ModelBatch
+    if precision is None:
+        precision = abi.PRECISION_FP64_STAGED
+    dev = torch.device("cuda", local)
+    specs = synth.model_batch_specs(nmodels, cells, seed=seed)
+    ins = []
+    for k, (nc, eos, n) in enumerate(specs):
+        P, T, z, sal = synth.model_points(nc, n, seed=1000 + k)
+        t = [torch.as_tensor(x, device=dev) for x in (P, T, z)]
+        if eos == "sw":
+            t.append(torch.as_tensor(sal, device=dev))
+        ins.append(tuple(t))
+    total = sum(n for _, _, n in specs)
+    mb = ModelBatch([model_fluid(nc, eos) for nc, eos, _ in specs], [n for _, _, n in specs], device=local)
+    t0 = time.perf_counter()
+    chosen = mb.tune(ins, precision, sample_points=4096)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t0
+    outs = mb.allocate()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    mb.flash(ins, precision, outs)   # capture
+    torch.cuda.synchronize()
+    grouped_ms = timed(lambda: mb.flash(ins, precision, outs))
+    evals = mb.eos_eval_count()
+    check_words = mb.self_check()
+    ctxs = [CubicThreePhaseFlash(model_fluid(nc, eos), device=local) for nc, eos, _ in specs]
+    souts = [c.allocate(n) for c, (_, _, n) in zip(ctxs, specs)]
+
+    def separate():
+        for c, inp, o, (_, _, n) in zip(ctxs, ins, souts, specs):
+            if n:
+                c.flash(inp[0], inp[1], inp[2], salinity=inp[3] if len(inp) > 3 else None,
+                        precision=precision, out=o)
+
+    separate()
+    torch.cuda.synchronize()
+    separate_ms = timed(separate)
+    mismatch = sum(int((outs[k]["presence"] != souts[k]["presence"]).sum().item()) +
+                   int((outs[k]["status"] != souts[k]["status"]).sum().item()) for k in range(len(specs)))
+    by_eos = {}
+    for nc, eos, n in specs:
+        by_eos[eos] = by_eos.get(eos, 0) + n
+    groups = sorted({nc for nc, _, n in specs if n > 0})
+    res = {
+        "models": nmodels, "cells": total, "cells_by_eos": by_eos,
+        "cell_range": f"log-uniform [{cells[0]:.0e}, {cells[1]:.0e}]",
+        "component_counts": groups,
+        "grouped": {"ms": grouped_ms, "cell_evals_per_s": total / (grouped_ms * 1e-3),
+                    "eos_evals_per_cell": evals / max(total, 1), "graph": "one captured CUDA graph",
+                    "kernel_launches": len(groups) * (staged_launches("fp64_staged") + 2) + 2,
+                    "self_check": {"queue_bound": check_words[0], "spin_guard": check_words[1]}},
+        "separate": {"ms": separate_ms, "cell_evals_per_s": total / (separate_ms * 1e-3),
+                     "kernel_launches": sum(1 for _, _, n in specs if n) * staged_launches("fp64_staged")},
+        "grouped_over_separate": separate_ms / grouped_ms,
+        "label_or_status_mismatch_vs_separate": mismatch,
+        "autotuner": {"chosen_blocks_per_sm": {str(nc): {"lane": v[0], "warp": v[1]} for nc, v in chosen.items()},
+                      "seconds": tune_s, "sample_points_per_nc": 4096},
+    }
+    mb.close()
+    return res
+
+
 def cpa_assembly_measure(local, shape, hbm_peak, relperm, timed, block=(20, 20)):
     """Residual + BAIJ Jacobian assembly of one Newton iterate on the
     200x200x50 hydrostatic grid with the six-component PR-CPA fluid (B = 19),
@@ -673,6 +755,11 @@ def run_gpu(args):
     if rank == 0 and args.serving_requests > 0:
         serving_stats = serving_measure(local, args.serving_requests)
 
+    multi_model = None
+    if rank == 0 and args.models > 0:
+        lo, hi = (float(v) for v in args.model_cells.split(","))
+        multi_model = models_measure(local, args.models, (lo, hi))
+
     natural = None
     if rank == 0 and not args.no_natural:
         try:
@@ -735,6 +822,7 @@ def run_gpu(args):
             "cpu_baseline": cpu,
             "natural": natural,
             "serving": serving_stats,
+            "multi_model": multi_model,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -762,6 +850,10 @@ def main():
                     help="skip the Natural Newton-evaluation measurements")
     ap.add_argument("--serving-requests", type=int, default=24,
                     help="requests of the serving-loop measurement (0 skips it)")
+    ap.add_argument("--models", type=int, default=256,
+                    help="models of the uneven multi-model batch measurement (0 skips it)")
+    ap.add_argument("--model-cells", default="1000,10000",
+                    help="cell-count range lo,hi (log-uniform) of the multi-model batch")
     ap.add_argument("--no-cpa-natural", action="store_true",
                     help="skip the six-component PR-CPA Natural grid")
     args = ap.parse_args()

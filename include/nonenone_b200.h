@@ -249,6 +249,55 @@ int nz_flash_batch_noalloc(nz_ctx* ctx, int64_t n, const double* pressure,
                            const double* salinity, const nz_flash_out* out,
                            int32_t precision, void* stream);
 
+/* ---- uneven multi-model batches -------------------------------------------
+ * A host running many independent models (a fluid and its cells each) calls
+ * CubicThreePhaseFlash::flash (three_phase_flash.hpp:83-227) per cell of each
+ * model; on the device that is one nz_flash_batch per model.  nz_models runs
+ * them together: the models of one component count share one staged launch
+ * sequence (each point reads its model's fluid from a device table, so PR, SW
+ * and PR-CPA models mix in the same kernels), the component-count groups run
+ * on forked streams, and the whole call -- upload of the callers' pointers,
+ * gather into group buffers, the staged kernels, scatter back -- is captured
+ * once into a CUDA graph and replayed on every later call.  Each model's
+ * answers are those of nz_flash_batch on that model alone.
+ *
+ * Point counts are fixed at creation (they size the group buffers and the
+ * graph).  Precision: NZ_PRECISION_FP64_STAGED or NZ_PRECISION_MIXED.
+ * Not thread safe; calls on one object are serialised by the caller.
+ */
+typedef struct nz_models nz_models;
+
+typedef struct nz_model_io {
+    const double* pressure;      /* [n] device */
+    const double* temperature;   /* [n] device */
+    const double* z;             /* [nc*n] device, component-major */
+    const double* salinity;      /* [n] device, or NULL: the fluid's sw_salinity */
+    nz_flash_out out;            /* the model's outputs (NULL fields are skipped) */
+} nz_model_io;
+
+/* options: NULL (defaults) or one per model. */
+int nz_models_create(int32_t nmodels, const nz_fluid_desc* fluids,
+                     const nz_flash_options* options, const int64_t* points,
+                     int32_t device, nz_models** out);
+int nz_models_destroy(nz_models* m);
+int nz_models_flash(nz_models* m, const nz_model_io* io, int32_t precision, void* stream);
+/* The autotuner: for every component count present, time the group's staged
+ * sequence on a strided sample of its points (up to sample_points) for each
+ * candidate launch shape and keep the fastest (the next nz_models_flash
+ * captures a new graph).  Synchronises the stream. */
+int nz_models_tune(nz_models* m, const nz_model_io* io, int32_t precision,
+                   int64_t sample_points, void* stream);
+/* Launch shape of a component count: resident blocks per SM of the lane
+ * kernels and of the warp-per-point kernels. */
+int nz_models_get_tuning(nz_models* m, int32_t nc, int32_t* lane_blocks_per_sm,
+                         int32_t* warp_blocks_per_sm);
+int nz_models_set_tuning(nz_models* m, int32_t nc, int32_t lane_blocks_per_sm,
+                         int32_t warp_blocks_per_sm);
+/* Self-check words of the last call (largest code over the groups). */
+int nz_models_check(nz_models* m, int32_t* bound_code, int32_t* guard_code);
+/* EOS evaluations of the last call (read after a stream sync). */
+int nz_models_eos_eval_count(nz_models* m, uint64_t* count);
+
 /* ---- tangent-plane stability ----------------------------------------------
  * Replaces CubicThreePhaseFlash::stabilityTest (three_phase_flash.hpp:300-489)
  * for a batch.  active[n] PhasePresence bits of the tested set,

@@ -111,6 +111,17 @@ class FlashOut(C.Structure):
     ]
 
 
+class ModelIO(C.Structure):
+    """nz_model_io: one model's device inputs and outputs."""
+    _fields_ = [
+        ("pressure", C.c_void_p),
+        ("temperature", C.c_void_p),
+        ("z", C.c_void_p),
+        ("salinity", C.c_void_p),
+        ("out", FlashOut),
+    ]
+
+
 class RelpermDesc(C.Structure):
     _fields_ = [
         ("swc", C.c_double), ("sorw", C.c_double), ("sgc", C.c_double),

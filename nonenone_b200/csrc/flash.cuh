@@ -61,6 +61,31 @@ struct Result
     }
 };
 
+#ifdef __CUDA_ARCH__
+// `out` on every lane of the warp = `r` of lane `src` (all lanes call it).
+template <int NC>
+__device__ void shuffleResult(const Result<NC> &r, int src, Result<NC> &out)
+{
+    out.converged = __shfl_sync(0xffffffffu, int(r.converged), src) != 0;
+    out.iterations = __shfl_sync(0xffffffffu, r.iterations, src);
+    out.presence = uint8_t(__shfl_sync(0xffffffffu, int(r.presence), src));
+    for (int p = 0; p < 3; ++p)
+    {
+        out.beta[p] = __shfl_sync(0xffffffffu, r.beta[p], src);
+        out.sat[p] = __shfl_sync(0xffffffffu, r.sat[p], src);
+        out.Z[p] = __shfl_sync(0xffffffffu, r.Z[p], src);
+        out.rho[p] = __shfl_sync(0xffffffffu, r.rho[p], src);
+        for (int i = 0; i < NC; ++i)
+            out.x[p][i] = __shfl_sync(0xffffffffu, r.x[p][i], src);
+    }
+    for (int i = 0; i < NC; ++i)
+    {
+        out.Kg[i] = __shfl_sync(0xffffffffu, r.Kg[i], src);
+        out.Kw[i] = __shfl_sync(0xffffffffu, r.Kw[i], src);
+    }
+}
+#endif
+
 // Outcome of one pressure-continuation anchor.
 constexpr int CONT_NONE = 0;
 constexpr int CONT_SUCCESS = 1;
@@ -2917,72 +2942,179 @@ struct Solver
         }
     }
 
-    // flashThreeAllocationFallback_ (allocation.inc:609-700).  The 23 seeds
-    // are built and processed in the reference's order; seed construction is
-    // independent of the processing, so it is done lazily per seed.
-    NZ_HDN void allocationFallback(double P, double T, const double *z, Result<NC> &best)
+    // One seed of flashThreeAllocationFallback_ (allocation.inc:609-700):
+    // build seed k (of 23, in the reference's order), precondition and refine
+    // it.  True when it ends in an admissible three-phase allocation (`state`
+    // holds it, with its Gibbs energy).
+    NZ_HDN bool allocationSeedState(double P, double T, const double *z, int k, AllocState &state)
     {
-        best.init();
-        double bestG = nzInf();
         const uint8_t pairs[3] = {OIL_BIT | GAS_BIT, OIL_BIT | WATER_BIT, GAS_BIT | WATER_BIT};
         const double thermo[6][3] = {{1.0, 0.0, 0.0}, {0.5, 0.0, 0.0}, {1.5, 0.0, 0.0},
                                      {1.0, -1.5, -1.5}, {1.0, 1.5, -1.5}, {1.0, -1.5, 1.5}};
         const double generic[12][2] = {{0.0, 0.0}, {1.0, -2.0}, {2.0, -4.0}, {2.0, -2.0},
                                        {1.0, -4.0}, {-1.0, -1.0}, {-2.0, -2.0}, {-2.0, 1.0},
                                        {-1.0, 2.0}, {2.0, 1.0}, {1.0, 2.0}, {-2.0, 2.0}};
+        double u[2 * NC];
+        bool valid = true;
+        if (k == 0)
+            valid = allocationSeedFromRawOg(P, T, z, u);
+        else if (k == 1)
+            valid = allocationSeedFromSingle(P, T, z, u);
+        else if (k < 5)
+            valid = allocationSeedFromPair(P, T, z, pairs[k - 2], u);
+        else if (k < 11)
+            thermodynamicAllocationSeed(P, T, thermo[k - 5][0], thermo[k - 5][1], thermo[k - 5][2], u);
+        else
+            for (int c = 0; c < NC; ++c)
+            {
+                u[c] = generic[k - 11][0];
+                u[NC + c] = generic[k - 11][1];
+            }
+        if (!valid)
+            return false;
+        gibbsPrecondition(P, T, z, u, state);
+        if (!state.valid)
+            return false;
+        if (!refineAllocation(P, T, z, u, state))
+            return false;
+        return state.beta[0] > O().betaTol && state.beta[1] > O().betaTol && state.beta[2] > O().betaTol;
+    }
+
+    // The three-phase result of an accepted allocation.
+    NZ_HDN void allocationCandidate(double P, double T, const AllocState &state, Result<NC> &cand)
+    {
+        cand.init();
+        cand.converged = true;
+        cand.presence = ALL_BITS;
+        for (int p = 0; p < 3; ++p)
+        {
+            cand.beta[p] = state.beta[p];
+            cand.Z[p] = state.Z[p];
+            for (int c = 0; c < NC; ++c)
+                cand.x[p][c] = state.x[p][c];
+        }
+        deriveReferenceK(cand);
+        updateSaturations(P, T, cand);
+    }
+
+    static constexpr int kAllocationSeeds = 23;
+
+    // flashThreeAllocationFallback_ (allocation.inc:609-700): the seeds in
+    // order, a seed replacing the best only with a strictly lower Gibbs
+    // energy; the first error ends the search.  The answer is therefore the
+    // first seed that reaches the lowest energy among the admissible ones,
+    // which lets warp-cooperative lanes run one seed each
+    // (allocationFallbackWarp) and reproduce it.
+    NZ_HDN void allocationFallback(double P, double T, const double *z, Result<NC> &best)
+    {
+        best.init();
+#ifdef __CUDA_ARCH__
+        if (width > 1)
+        {
+            allocationFallbackWarp(P, T, z, best);
+            return;
+        }
+#endif
+        double bestG = nzInf();
         AllocState state;
         Result<NC> cand;
 #pragma unroll 1
-        for (int k = 0; k < 23; ++k)
+        for (int k = 0; k < kAllocationSeeds; ++k)
         {
             if (err)
                 return;
-            double u[2 * NC];
-            bool valid = true;
-            if (k == 0)
-                valid = allocationSeedFromRawOg(P, T, z, u);
-            else if (k == 1)
-                valid = allocationSeedFromSingle(P, T, z, u);
-            else if (k < 5)
-                valid = allocationSeedFromPair(P, T, z, pairs[k - 2], u);
-            else if (k < 11)
-                thermodynamicAllocationSeed(P, T, thermo[k - 5][0], thermo[k - 5][1], thermo[k - 5][2], u);
-            else
-                for (int c = 0; c < NC; ++c)
-                {
-                    u[c] = generic[k - 11][0];
-                    u[NC + c] = generic[k - 11][1];
-                }
-            if (!valid)
-                continue;
-            gibbsPrecondition(P, T, z, u, state);
-            if (!state.valid)
-                continue;
-            if (!refineAllocation(P, T, z, u, state))
-                continue;
-            if (!(state.beta[0] > O().betaTol) || !(state.beta[1] > O().betaTol) ||
-                !(state.beta[2] > O().betaTol))
+            if (!allocationSeedState(P, T, z, k, state))
                 continue;
             if (!(state.gibbs < bestG))
                 continue;
-            cand.init();
-            cand.converged = true;
-            cand.presence = ALL_BITS;
-            for (int p = 0; p < 3; ++p)
-            {
-                cand.beta[p] = state.beta[p];
-                cand.Z[p] = state.Z[p];
-                for (int c = 0; c < NC; ++c)
-                    cand.x[p][c] = state.x[p][c];
-            }
-            deriveReferenceK(cand);
-            updateSaturations(P, T, cand);
+            allocationCandidate(P, T, state, cand);
             if (!cand.converged)
                 continue;
             best = cand;
             bestG = state.gibbs;
         }
     }
+
+#ifdef __CUDA_ARCH__
+    // Lane k runs seed k alone (width 1, its own error flag); the warp then
+    // replays the sequential acceptance over the seeds' outcomes in order and
+    // takes the chosen candidate from its lane.  A candidate's saturation
+    // update runs on its lane whether or not the sequential loop would reach
+    // it; its error only counts where the loop would have run it.
+    NZ_HDN void allocationFallbackWarp(double P, double T, const double *z, Result<NC> &best)
+    {
+        static_assert(kAllocationSeeds <= 32, "one allocation seed per lane");
+        if (err)
+            return;
+        const int savedWidth = width;
+        const int savedLane = lane;
+        const unsigned long long evals0 = evals;
+        width = 1;
+        lane = 0;
+        bool admissible = false;
+        bool candidateOk = false;
+        int seedErr = ERR_NONE;
+        int candErr = ERR_NONE;
+        double g = 0.0;
+        Result<NC> mine;
+        mine.init();
+        if (savedLane < kAllocationSeeds)
+        {
+            AllocState state;
+            admissible = allocationSeedState(P, T, z, savedLane, state);
+            seedErr = err;
+            err = ERR_NONE;
+            if (admissible && seedErr == ERR_NONE)
+            {
+                g = state.gibbs;
+                allocationCandidate(P, T, state, mine);
+                candErr = err;
+                err = ERR_NONE;
+                candidateOk = mine.converged;
+            }
+        }
+        width = savedWidth;
+        lane = savedLane;
+        __syncwarp();
+        unsigned long long spent = evals - evals0;
+        for (int off = 16; off > 0; off >>= 1)
+            spent += __shfl_xor_sync(0xffffffffu, spent, off);
+        evals = evals0 + spent;
+        double bestG = nzInf();
+        int bestK = -1;
+        int code = ERR_NONE;
+#pragma unroll 1
+        for (int k = 0; k < kAllocationSeeds; ++k)
+        {
+            const int ek = __shfl_sync(0xffffffffu, seedErr, k);
+            const bool ok = __shfl_sync(0xffffffffu, int(admissible), k) != 0;
+            const double gk = __shfl_sync(0xffffffffu, g, k);
+            const int ck = __shfl_sync(0xffffffffu, candErr, k);
+            const bool conv = __shfl_sync(0xffffffffu, int(candidateOk), k) != 0;
+            if (ek != ERR_NONE)
+            {
+                code = ek;
+                break;
+            }
+            if (!ok || !(gk < bestG))
+                continue;
+            if (ck != ERR_NONE)
+            {
+                bestK = k;
+                code = ck;
+                break;
+            }
+            if (!conv)
+                continue;
+            bestK = k;
+            bestG = gk;
+        }
+        if (code != ERR_NONE)
+            fail(code);
+        if (bestK >= 0)
+            shuffleResult(mine, bestK, best);
+    }
+#endif
 
     // ------------------------------------------------------- active set ----
     // equilibrateActiveSet_ (allocation.inc:707-858)

@@ -40,6 +40,24 @@ int stagedLaunchExt(const FluidDev &F, void *scratch, int64_t n, const double *P
 {
     return stagedLaunch<NC>(F, scratch, n, P, T, z, sal, out, evalCounter, smCount, st, mixed);
 }
+// The staged launch sequence of a multi-model batch: per-point fluids from
+// `fluids` (indexed by `model`), launch shape from the caller's tuning.
+template <int NC>
+int stagedLaunchModel(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
+                      const double *z, const double *sal, const nz_flash_out &out,
+                      unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed, int *check,
+                      int laneBlocksPerSm, int warpBlocksPerSm, const FluidDev *fluids, const uint16_t *model)
+{
+    StagedTuning tune;
+    tune.laneBlocksPerSm = laneBlocksPerSm;
+    tune.warpBlocksPerSm = warpBlocksPerSm;
+    return stagedLaunch<NC>(F, scratch, n, P, T, z, sal, out, evalCounter, smCount, st, mixed, check, tune, fluids,
+                            model);
+}
+template int stagedLaunchModel<NZ_INST_NC>(const FluidDev &, void *, int64_t, const double *, const double *,
+                                           const double *, const double *, const nz_flash_out &,
+                                           unsigned long long *, int, cudaStream_t, bool, int *, int, int,
+                                           const FluidDev *, const uint16_t *);
 template int stagedLaunchExt<NZ_INST_NC>(const FluidDev &, void *, int64_t, const double *, const double *,
                                          const double *, const double *, const nz_flash_out &,
                                          unsigned long long *, int, cudaStream_t, bool);

@@ -75,7 +75,21 @@ struct StagedArgs
     int64_t contCap;
     unsigned long long *evalCounter;
     int mixed;   // TPD trials: mixed-precision leading SSI steps
+    // Multi-model batches: the fluid of each model and the model of each point
+    // (null: every point uses the kernels' own fluid argument).
+    const FluidDev *fluids;
+    const uint16_t *model;
 };
+
+// The fluid point i is flashed with, and its salinity.
+__device__ __forceinline__ const FluidDev *pointFluid(const FluidDev &F, const StagedArgs &a, int64_t i)
+{
+    return a.fluids ? a.fluids + a.model[i] : &F;
+}
+__device__ __forceinline__ double pointSalinity(const FluidDev &F, const StagedArgs &a, int64_t i)
+{
+    return a.sal ? a.sal[i] : pointFluid(F, a, i)->salinity;
+}
 
 // Per-round counters for the active-set rounds and the recovery rounds, then
 // the shared ones.
@@ -205,8 +219,8 @@ stagedStartKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
         Driver<NC> d;
         d.st = &states[i];
-        const double sal = a.sal ? a.sal[i] : F.salinity;
-        d.s.setup(&F, sal);
+        const double sal = pointSalinity(F, a, i);
+        d.s.setup(pointFluid(F, a, i), sal);
         d.st->sal = sal;
         double zi[NC];
         for (int c = 0; c < NC; ++c)
@@ -245,7 +259,7 @@ stagedClassifyKernel(const __grid_constant__ FluidDev F, const __grid_constant__
         const TrialOut<NC> *trials = static_cast<const TrialOut<NC> *>(a.trials) + i * 3 * nseeds;
         Driver<NC> d;
         d.st = &states[i];
-        d.s.setup(&F, d.st->sal);
+        d.s.setup(pointFluid(F, a, i), d.st->sal);
         d.combineStability(trials, nseeds, d.st->sr);
         d.st->err = d.s.err;   // a trial error ends the active-set path on resume
         bool adds = false;
@@ -281,7 +295,7 @@ stagedResumeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
         Driver<NC> d;
         d.st = &states[i];
-        d.s.setup(&F, d.st->sal);
+        d.s.setup(pointFluid(F, a, i), d.st->sal);
         d.s.err = d.st->err;
         const StabilityResult<NC> sr = d.st->sr;
         const uint8_t stage = d.activeSetLoop(true, &sr);
@@ -358,7 +372,7 @@ stagedThreeKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                     {
                         const DriverState<NC> &st = states[i];
                         evals += s.evals;
-                        s.setup(&F, st.sal);
+                        s.setup(pointFluid(F, a, i), st.sal);
                         kind = int(task & 1u);
                         if (kind == 1)
                             s.memo = reinterpret_cast<const Rr3Memo<NC> *>(static_cast<const TrialOut<NC> *>(a.trials) +
@@ -441,7 +455,7 @@ stagedThreeLongKernel(const __grid_constant__ FluidDev F, const __grid_constant_
         DriverState<NC> &st = states[i];
         const int kind = int(task & 1u);
         Solver<NC> s;
-        s.setup(&F, st.sal);
+        s.setup(pointFluid(F, a, i), st.sal);
         s.lane = lane;
         s.width = 32;
         if (kind == 1)
@@ -489,7 +503,7 @@ stagedThreeResumeKernel(const __grid_constant__ FluidDev F, const __grid_constan
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
         Driver<NC> d;
         d.st = &states[i];
-        d.s.setup(&F, d.st->sal);
+        d.s.setup(pointFluid(F, a, i), d.st->sal);
         d.s.err = d.st->err;
         const uint8_t stage = d.activeSetLoop(false, nullptr, true);
         routePoint<NC>(a, out, round + 1, i, stage, d);
@@ -554,7 +568,7 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                         atomicExch(&a.counters[kCounterBound], 5);
                     const DriverState<NC> &st = states[bad ? 0 : point];
                     evals += s.evals;
-                    s.setup(&F, st.sal);
+                    s.setup(pointFluid(F, a, bad ? 0 : point), st.sal);
                     s.mixed = a.mixed != 0;
                     L.P = st.P;
                     L.T = st.T;
@@ -696,7 +710,7 @@ stagedRr3MemoKernel(const __grid_constant__ FluidDev F, const __grid_constant__ 
         if (!st.mainFailed)
             continue;
         Solver<NC> s;
-        s.setup(&F, st.sal);
+        s.setup(pointFluid(F, a, i), st.sal);
         Rr3Memo<NC> m;
         double kg[NC], kw[NC];
         s.wilsonK(st.P, st.T, kg);
@@ -808,7 +822,7 @@ stagedRecoverStartKernel(const __grid_constant__ FluidDev F, const __grid_consta
                 atomicExch(&a.counters[kCounterBound], 12);
             continue;
         }
-        d.s.setup(&F, d.st->sal);
+        d.s.setup(pointFluid(F, a, i), d.st->sal);
         d.recoveryOneStart();
         const int t = atomicAdd(&a.counters[kCounterThree], 1);
         if (t < a.n)
@@ -841,7 +855,7 @@ stagedRecoverThreeKernel(const __grid_constant__ FluidDev F, const __grid_consta
         DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
         Driver<NC> d;
         d.st = &states[i];
-        d.s.setup(&F, d.st->sal);
+        d.s.setup(pointFluid(F, a, i), d.st->sal);
         d.s.err = d.st->err;
         Result<NC> full = d.st->lastPhysical;
         if (d.s.err || d.recoveryOneAccept(full))
@@ -893,7 +907,7 @@ stagedRecoverResumeKernel(const __grid_constant__ FluidDev F, const __grid_const
         const TrialOut<NC> *trials = static_cast<const TrialOut<NC> *>(a.trials) + i * 3 * nseeds;
         Driver<NC> d;
         d.st = &states[i];
-        d.s.setup(&F, d.st->sal);
+        d.s.setup(pointFluid(F, a, i), d.st->sal);
         d.reducedCombine(trials, nseeds);
         const uint8_t stage = d.s.err ? STAGE_DONE : d.reducedAdvance();
         routeRecovery<NC>(a, out, rr + 1, i, stage, d);
@@ -928,7 +942,7 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
             continue;
         }
         Solver<NC> s;
-        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
         s.lane = lane;
         s.width = 32;
         double zi[NC];
@@ -1022,7 +1036,7 @@ stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
             continue;
         }
         Solver<NC> s;
-        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
         s.lane = lane;
         s.width = 32;
         double zn[NC];
@@ -1085,7 +1099,7 @@ stagedSelectKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
             continue;
         }
         Solver<NC> s;
-        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
         s.lane = lane;
         s.width = 32;
         double zn[NC];
@@ -1134,7 +1148,7 @@ stagedPolishKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
         if (out.status[i] != NZ_FLASH_CONVERGED || popcount3(pres) < 2)
             continue;
         Solver<NC> s;
-        s.setup(&F, a.sal ? a.sal[i] : F.salinity);
+        s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
         double zn[NC];
         for (int c = 0; c < NC; ++c)
             zn[c] = a.z[c * a.n + i];
@@ -1227,6 +1241,15 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
     return a;
 }
 
+// Launch shape of the staged kernels: resident blocks per SM of the lane
+// kernels (TPD trials, three-phase step machine) and of the warp-per-point
+// kernels.  The multi-model path picks them per component count by timing.
+struct StagedTuning
+{
+    int laneBlocksPerSm = kTrialBlocksPerSm;
+    int warpBlocksPerSm = 8;
+};
+
 // Launch sequence of one staged flash on `st`; the scratch block must hold
 // stagedScratchBytes<NC>(n) bytes.  No allocation, no host synchronisation.
 // `check` (null or two device ints) receives the batch's queue-bound and
@@ -1236,10 +1259,14 @@ template <int NC>
 int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
                  const double *z, const double *sal, const nz_flash_out &out,
                  unsigned long long *evalCounter, int smCount, cudaStream_t st, bool mixed = false,
-                 int *check = nullptr)
+                 int *check = nullptr, const StagedTuning &tune = StagedTuning(),
+                 const FluidDev *fluids = nullptr, const uint16_t *model = nullptr)
 {
     StagedArgs a = stagedCarve<NC>(scratch, n, F);
     a.mixed = mixed ? 1 : 0;
+    a.fluids = fluids;
+    a.model = model;
+    const unsigned warpGrid = unsigned(smCount * tune.warpBlocksPerSm);
     a.P = P;
     a.T = T;
     a.z = z;
@@ -1263,7 +1290,7 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     stagedStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     if (after("start", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed after start");
-    const unsigned trialGrid = unsigned(smCount * kTrialBlocksPerSm);
+    const unsigned trialGrid = unsigned(smCount * tune.laneBlocksPerSm);
     for (int round = 0; round + 1 < kMaxRounds; ++round)
     {
         stagedTrialKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a, round);
@@ -1273,16 +1300,16 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         stagedResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round, 0);
         stagedResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round, 1);
         stagedThreeKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a);
-        stagedThreeLongKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
+        stagedThreeLongKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a);
         stagedThreeResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, round);
         stagedResetSplitKernel<<<1, 1, 0, st>>>(a.counters);
         if (after("resume", round + 1))
             return setError(NZ_ERR_CUDA, "staged flash self-check failed in resume");
     }
-    stagedRr3MemoKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
+    stagedRr3MemoKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a);
     stagedRecoverStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     stagedThreeKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a);
-    stagedThreeLongKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a);
+    stagedThreeLongKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a);
     stagedRecoverThreeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     if (after("recover", kMaxRounds))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
@@ -1293,14 +1320,14 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         if (after("recover round", kMaxRounds + rr + 1))
             return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
     }
-    stagedFullKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, out);
+    stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out);
     if (after("full", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the full solver");
     // one launch per anchor, each for the points no earlier anchor decided:
     // the work is the fallback's own (it stops at the first anchor with an
     // outcome), the points run side by side
     for (int an = 0; an < kAnchors; ++an)
-        stagedAnchorKernel<NC><<<unsigned(smCount * 8), kFlashBlock, 0, st>>>(F, a, an, 1);
+        stagedAnchorKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, an, 1);
     stagedSelectKernel<NC><<<unsigned(smCount * 2), kFlashBlock, 0, st>>>(F, a, out);
     if (after("continuation", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the pressure continuation");

@@ -21,6 +21,8 @@ EXPORTED = (
     "nz_update_state", "nz_residual", "nz_jacobian", "nz_diag_fma_peak",
     "nz_flash_batch_noalloc", "nz_natural_init_ptz", "nz_natural_set_update_mode",
     "nz_flash_check", "nz_ctx_set_spin_limit", "nz_jacobian_columns",
+    "nz_models_create", "nz_models_destroy", "nz_models_flash", "nz_models_tune",
+    "nz_models_get_tuning", "nz_models_set_tuning", "nz_models_check", "nz_models_eos_eval_count",
 )
 
 _lib = None
@@ -65,6 +67,14 @@ def load():
     L.nz_flash_batch_noalloc.argtypes = [vp, i64, vp, vp, vp, vp, vp, i32, vp]
     L.nz_flash_check.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
     L.nz_ctx_set_spin_limit.argtypes = [vp, i64]
+    L.nz_models_create.argtypes = [i32, vp, vp, vp, i32, C.POINTER(vp)]
+    L.nz_models_destroy.argtypes = [vp]
+    L.nz_models_flash.argtypes = [vp, vp, i32, vp]
+    L.nz_models_tune.argtypes = [vp, vp, i32, i64, vp]
+    L.nz_models_get_tuning.argtypes = [vp, i32, C.POINTER(i32), C.POINTER(i32)]
+    L.nz_models_set_tuning.argtypes = [vp, i32, i32, i32]
+    L.nz_models_check.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.nz_models_eos_eval_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     if L.nz_abi_version() != 2:
         raise NzError("ABI version mismatch")
     _lib = L

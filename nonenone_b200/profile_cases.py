@@ -1,6 +1,6 @@
 """Single workloads to run under a profiler (one process, one GPU).
 
-  python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged|mixed]
+  python -m nonenone_b200.profile_cases flash N [--precision fp64|fp64_staged|mixed] [--eos pr|sw]
       one N-point batch of the seeded flash mixture (after a 4,096-point warm-up
       batch, so kernels of the measured batch come second)
   python -m nonenone_b200.profile_cases natural NX NY NZ [--update] [--per-cell] [--fluid pr3|cpa6]
@@ -17,21 +17,29 @@ import sys
 import numpy as np
 
 
-def run_flash(n: int, precision: str) -> None:
+def run_flash(n: int, precision: str, eos: str = "pr") -> None:
     import torch
     from . import abi, synth
     from .flash import CubicThreePhaseFlash
     from .fluids import make_fluid
     prec = {"fp64": abi.PRECISION_FP64, "fp64_staged": abi.PRECISION_FP64_STAGED,
             "mixed": abi.PRECISION_MIXED}[precision]
-    fl = CubicThreePhaseFlash(make_fluid())
-    P, T, z = synth.flash_points(n, seed=1)
-    fl.flash(P[:4096], T[:4096], np.ascontiguousarray(z[:, :4096]), precision=prec)
+    if eos == "sw":
+        fl = CubicThreePhaseFlash(make_fluid(eos_model=abi.EOS_SW, salinity=1.0))
+        P, T, z, sal = synth.flash_points(n, seed=2, salinity=True)
+    else:
+        fl = CubicThreePhaseFlash(make_fluid())
+        P, T, z = synth.flash_points(n, seed=1)
+        sal = None
+    w = min(n, 4096)
+    fl.flash(P[:w], T[:w], np.ascontiguousarray(z[:, :w]), precision=prec,
+             salinity=None if sal is None else sal[:w])
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dP, dT, dz = (torch.as_tensor(x, device=fl.device) for x in (P, T, z))
+    dsal = None if sal is None else torch.as_tensor(sal, device=fl.device)
     out = fl.allocate(n)
     a.record()
-    fl.flash(dP, dT, dz, precision=prec, out=out)
+    fl.flash(dP, dT, dz, precision=prec, out=out, salinity=dsal)
     b.record()
     torch.cuda.synchronize()
     print(f"flash {n} points: {a.elapsed_time(b):.1f} ms, status counts "
@@ -112,6 +120,8 @@ def main(argv=None) -> int:
     f = sub.add_parser("flash")
     f.add_argument("n", type=int)
     f.add_argument("--precision", default="fp64_staged", choices=["fp64", "fp64_staged", "mixed"])
+    f.add_argument("--eos", default="pr", choices=["pr", "sw"],
+                   help="PR, or Soreide-Whitson with salinity ~ U[0,2] mol/kg")
     nat = sub.add_parser("natural")
     nat.add_argument("nx", type=int)
     nat.add_argument("ny", type=int)
@@ -123,7 +133,7 @@ def main(argv=None) -> int:
     nat.add_argument("--scale", type=float, default=1.0, help="perturbation scale of the updated iterate")
     a = ap.parse_args(argv)
     if a.case == "flash":
-        run_flash(a.n, a.precision)
+        run_flash(a.n, a.precision, a.eos)
     else:
         run_natural(a.nx, a.ny, a.nz, a.update, a.per_cell, a.fluid, a.scale)
     return 0

@@ -208,3 +208,38 @@ def perturb_natural_state(primary, phase_state, nc: int, seed: int, scale: float
         ph = present[rng.integers(len(present))]
         p[c, 1 + ncomp + ph] = 5.0e-5
     return p
+
+
+# Component counts and EOS families of the multi-model workload.
+MODEL_NCS = (3, 4, 5, 6, 8)
+MODEL_EOS = ("pr", "sw", "cpa")
+
+
+def model_batch_specs(nmodels: int, cells=(1.0e4, 5.0e5), seed: int = 21, eos=MODEL_EOS, eos_weights=None):
+    """The uneven multi-model workload: per model a cell count log-uniform on
+    `cells`, a component count uniform over MODEL_NCS and an EOS drawn from
+    `eos` (uniform, or with `eos_weights`).  Returns [(nc, eos, cells)]."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(cells[0]), np.log(cells[1])
+    n = np.exp(rng.uniform(lo, hi, nmodels)).astype(np.int64)
+    ncs = rng.choice(MODEL_NCS, nmodels)
+    kinds = rng.choice(len(eos), nmodels, p=eos_weights)
+    return [(int(c), eos[int(e)], int(m)) for c, e, m in zip(ncs, kinds, n)]
+
+
+def model_points(nc: int, n: int, seed: int, depth=(0.0, 250.0), p_top: float = 20.0e6,
+                 p_gradient: float = 0.01e6, t_top: float = 373.15, t_gradient: float = 0.03,
+                 salinity=(0.0, 2.0)):
+    """P, T, z of one model drawn as on the hydrostatic benchmark grid: a depth
+    uniform on `depth` m, P = 20 MPa + 0.01 MPa/m and T = 373.15 K + 0.03 K/m
+    of it, z ~ Dirichlet(4, 2, 1, ..., 1) over the model's nc components, and a
+    salinity U[0, 2] mol/kg (read by Soreide-Whitson models only).
+    Returns P[n], T[n], z[nc, n], salinity[n]."""
+    rng = np.random.default_rng(seed)
+    d = rng.uniform(depth[0], depth[1], n)
+    P = p_top + p_gradient * d
+    T = t_top + t_gradient * d
+    alpha = [4.0, 2.0] + [1.0] * (nc - 2)
+    z = np.ascontiguousarray(rng.dirichlet(alpha, n).T)
+    sal = rng.uniform(salinity[0], salinity[1], n)
+    return P, T, z, sal
