@@ -3,6 +3,7 @@
 
 #include "../../include/nonenone_b200.h"
 #include "eos.cuh"
+#include "fluid_dev.cuh"
 
 #include <cstdarg>
 #include <cuda_runtime.h>
@@ -14,8 +15,6 @@ constexpr int kFlashBlock = 128;
 // nz_ctx::evalCounter block: the EOS evaluation count (8 bytes), then the
 // last batch's two self-check words (queue bound, spin guard).
 constexpr size_t kCounterBlockBytes = 16;
-// Default iteration cap of the lane-refill loops (FluidDev::spinLimit).
-constexpr long long kDefaultSpinLimit = 1LL << 26;
 constexpr int kTrialBlock = 128;
 constexpr int kTrialBlocksPerSm = 8;
 

@@ -325,6 +325,44 @@ struct FlashMemo
     }
 };
 
+// What one seed of the SW allocation search ends in (computed ahead of time
+// by the staged batched flash, one lane per seed): admissible or not, the
+// error it raised, its Gibbs energy and the three-phase allocation.
+template <int NC>
+struct AllocSeedOut
+{
+    double gibbs;
+    double beta[3];
+    double Z[3];
+    double x[3][NC];
+    int admissible;
+    int err;
+};
+
+constexpr int kAllocSeedCount = 23;   // seeds of flashThreeAllocationFallback_ (allocation.inc:609-700)
+
+// The allocation search of one exact input (P, T, salinity, z): every seed's
+// outcome.  allocationFallback replays the sequential acceptance over them
+// when it is called with identical inputs and the default phase roles.
+template <int NC>
+struct AllocMemo
+{
+    double P, T, salinity;
+    double z[NC];
+    int valid;
+    AllocSeedOut<NC> seed[kAllocSeedCount];
+
+    NZ_HD bool matches(double p, double t, double s, const double *zz) const
+    {
+        if (!valid || P != p || T != t || salinity != s)
+            return false;
+        for (int i = 0; i < NC; ++i)
+            if (z[i] != zz[i])
+                return false;
+        return true;
+    }
+};
+
 // ============================================================================
 template <int NC>
 struct Solver
@@ -348,6 +386,7 @@ struct Solver
     const Rr3Memo<NC> *memo;   // optional precomputed rr3Robust answer
     StabilityMemo<NC> *stabMemo;   // optional precomputed stability test
     const FlashMemo<NC> *flashMemo;   // optional precomputed top-level flash
+    const AllocMemo<NC> *allocMemo;   // optional precomputed SW allocation seeds
     bool mixed;                    // mixed-precision successive substitution in the TPD trials
 
     NZ_HD void setup(const FluidDev *fluid, double s)
@@ -366,6 +405,7 @@ struct Solver
         memo = nullptr;
         stabMemo = nullptr;
         flashMemo = nullptr;
+        allocMemo = nullptr;
         mixed = false;
     }
 
@@ -2981,23 +3021,76 @@ struct Solver
     }
 
     // The three-phase result of an accepted allocation.
-    NZ_HDN void allocationCandidate(double P, double T, const AllocState &state, Result<NC> &cand)
+    NZ_HDN void allocationCandidate(double P, double T, const double (&beta)[3], const double (&Z)[3],
+                                    const double (&x)[3][NC], Result<NC> &cand)
     {
         cand.init();
         cand.converged = true;
         cand.presence = ALL_BITS;
         for (int p = 0; p < 3; ++p)
         {
-            cand.beta[p] = state.beta[p];
-            cand.Z[p] = state.Z[p];
+            cand.beta[p] = beta[p];
+            cand.Z[p] = Z[p];
             for (int c = 0; c < NC; ++c)
-                cand.x[p][c] = state.x[p][c];
+                cand.x[p][c] = x[p][c];
         }
         deriveReferenceK(cand);
         updateSaturations(P, T, cand);
     }
+    NZ_HDN void allocationCandidate(double P, double T, const AllocState &state, Result<NC> &cand)
+    {
+        allocationCandidate(P, T, state.beta, state.Z, state.x, cand);
+    }
 
-    static constexpr int kAllocationSeeds = 23;
+    // Seed k's outcome for an AllocMemo (run with width 1; err is left as it was).
+    NZ_HDN void allocationSeedOutcome(double P, double T, const double *z, int k, AllocSeedOut<NC> &o)
+    {
+        const int before = err;
+        err = ERR_NONE;
+        AllocState state;
+        const bool admissible = allocationSeedState(P, T, z, k, state);
+        o.err = err;
+        err = before;
+        o.admissible = admissible ? 1 : 0;
+        o.gibbs = admissible ? state.gibbs : 0.0;
+        for (int p = 0; p < 3; ++p)
+        {
+            o.beta[p] = admissible ? state.beta[p] : 0.0;
+            o.Z[p] = admissible ? state.Z[p] : 0.0;
+            for (int c = 0; c < NC; ++c)
+                o.x[p][c] = admissible ? state.x[p][c] : 0.0;
+        }
+    }
+
+    // The sequential acceptance over stored seed outcomes.  An error of seed
+    // k ends the search there (the caller returns on it, so `best` no longer
+    // matters).
+    NZ_HDN void allocationReplay(double P, double T, const AllocMemo<NC> &m, Result<NC> &best)
+    {
+        double bestG = nzInf();
+        Result<NC> cand;
+#pragma unroll 1
+        for (int k = 0; k < kAllocationSeeds; ++k)
+        {
+            if (err)
+                return;
+            const AllocSeedOut<NC> &o = m.seed[k];
+            if (o.err != ERR_NONE)
+            {
+                fail(o.err);
+                return;
+            }
+            if (!o.admissible || !(o.gibbs < bestG))
+                continue;
+            allocationCandidate(P, T, o.beta, o.Z, o.x, cand);
+            if (!cand.converged)
+                continue;
+            best = cand;
+            bestG = o.gibbs;
+        }
+    }
+
+    static constexpr int kAllocationSeeds = kAllocSeedCount;
 
     // flashThreeAllocationFallback_ (allocation.inc:609-700): the seeds in
     // order, a seed replacing the best only with a strictly lower Gibbs
@@ -3008,6 +3101,12 @@ struct Solver
     NZ_HDN void allocationFallback(double P, double T, const double *z, Result<NC> &best)
     {
         best.init();
+        if (allocMemo && roles[0] == OIL && roles[1] == GAS && roles[2] == WATER &&
+            allocMemo->matches(P, T, salinity, z))
+        {
+            allocationReplay(P, T, *allocMemo, best);
+            return;
+        }
 #ifdef __CUDA_ARCH__
         if (width > 1)
         {
@@ -3615,6 +3714,7 @@ struct Solver
                     continue;
                 Solver<NC> cand = *this;
                 cand.stabMemo = nullptr;   // stored tests were taken with the default roles
+                cand.allocMemo = nullptr;
                 cand.roles[0] = perm[0];
                 cand.roles[1] = perm[1];
                 cand.roles[2] = perm[2];

@@ -15,7 +15,6 @@
 
 namespace nz
 {
-FluidDev makeFluidDev(const nz_fluid_desc &d, const nz_flash_options &o);
 template <int NC>
 int stagedLaunchModel(const FluidDev &F, void *scratch, int64_t n, const double *P, const double *T,
                       const double *z, const double *sal, const nz_flash_out &out,
@@ -129,6 +128,11 @@ struct ModelGroup
     cudaEvent_t done{nullptr};
     int laneBlocksPerSm{kTrialBlocksPerSm};
     int warpBlocksPerSm{8};
+    // The fluid that sizes the group's work space and is passed as the
+    // kernels' own fluid argument: the first member's, marked SW when any
+    // member is SW (so the work space holds the SW allocation memos).  Every
+    // point still reads its own model's fluid from the table.
+    FluidDev shape{};
 };
 } // namespace nz
 
@@ -224,7 +228,7 @@ int allocGroupOutputs(ModelGroup &g)
 int launchGroup(const nz_models *m, int gi, int64_t count, bool mixed)
 {
     const ModelGroup &g = m->groups[gi];
-    const FluidDev &F = m->fluids[g.members[0]];
+    const FluidDev &F = g.shape;
     nz_flash_out out = g.out;
     // the staged kernels address the outputs with the batch size as stride
     const int64_t n = count;
@@ -380,7 +384,11 @@ extern "C" int nz_models_create(int32_t nmodels, const nz_fluid_desc *fluids, co
         rc = rc ? rc : allocGroupOutputs(G);
         if (rc)
             return fail(rc);
-        G.scratchBytes = stagedScratchBytesFor(nc, G.points, m->fluids[G.members[0]]);
+        G.shape = m->fluids[G.members[0]];
+        for (int k : G.members)
+            if (m->fluids[k].eosModel == NZ_EOS_SW)
+                G.shape.eosModel = NZ_EOS_SW;
+        G.scratchBytes = stagedScratchBytesFor(nc, G.points, G.shape);
         cudaError_t e = cudaMalloc(&G.scratch, G.scratchBytes);
         if (e != cudaSuccess)
             return fail(cudaFail(e, "nz_models: staged work space"));

@@ -59,6 +59,7 @@ struct DriverState
     double r2BestG;       // recovery 2: Gibbs energy of the best certified candidate (in `seed`)
     double threeKg[NC];   // starting K of the pending three-phase solve
     double threeKw[NC];
+    int allocSlot;        // SW allocation search precomputed in this memo slot (-1: none)
 };
 
 template <int NC>

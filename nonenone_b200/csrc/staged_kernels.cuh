@@ -79,6 +79,11 @@ struct StagedArgs
     // (null: every point uses the kernels' own fluid argument).
     const FluidDev *fluids;
     const uint16_t *model;
+    // SW allocation search ahead of the recovery kernel (SW batches only):
+    // AllocMemo<NC>[allocCap] and the point of each memo slot
+    void *allocMemos;
+    int *allocPoints;
+    int64_t allocCap;
 };
 
 // The fluid point i is flashed with, and its salinity.
@@ -104,6 +109,8 @@ constexpr int kCounterRest = kCounterFull + 5;
 constexpr int kCounterThree = kCounterFull + 6;        // queued three-phase solves
 constexpr int kCounterThreeCursor = kCounterFull + 7;  // refill cursor of the three-phase kernel
 constexpr int kCounterThreeLong = kCounterFull + 8;    // solves handed to the warp kernel
+constexpr int kCounterAlloc = kCounterFull + 9;        // points queued for the lane allocation search
+constexpr int kCounterAllocCursor = kCounterFull + 10; // its (point, seed) task cursor
 // Steps a lane of the three-phase kernel gives one solve before handing it to
 // the warp kernel.  Most solves end within ~40 steps; the few long ones are
 // long because their robust Rachford-Rice solves fail start after start,
@@ -128,6 +135,17 @@ inline int64_t contCapacity(int64_t n)
     if (n <= 64)
         return n;
     return n / 32 < 64 ? 64 : n / 32;
+}
+
+// Memo slots of the lane allocation search (SW batches): an eighth of the
+// points (the search is reached by ~7 % of a typical SW batch); points past it
+// run the search inside the recovery kernel.
+inline int64_t allocCapacity(int64_t n, const FluidDev &F)
+{
+    if (F.eosModel != EOS_SW)
+        return 0;
+    const int64_t cap = n / 8 + 256;
+    return cap < n ? cap : n;
 }
 
 // A queue bound or a spin guard has tripped in this batch: the kernels that
@@ -916,6 +934,83 @@ stagedRecoverResumeKernel(const __grid_constant__ FluidDev F, const __grid_const
     warpAddEvals(a.evalCounter, evals);
 }
 
+// Rest points whose next recovery is the SW allocation search get a memo
+// slot, filled by stagedAllocSeedKernel before the recovery kernel runs;
+// points past the capacity run the search inside the recovery kernel.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedAllocQueueKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
+{
+    if (stagedTripped(a))
+        return;
+    const int count = a.counters[kCounterRest];
+    DriverState<NC> *states = static_cast<DriverState<NC> *>(a.states);
+    AllocMemo<NC> *memos = static_cast<AllocMemo<NC> *>(a.allocMemos);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count && k < a.n; k += gridDim.x * blockDim.x)
+    {
+        const int64_t i = a.split[0][k];
+        if (i < 0 || i >= a.n)
+        {
+            atomicExch(&a.counters[kCounterBound], 16);
+            continue;
+        }
+        DriverState<NC> &st = states[i];
+        st.allocSlot = -1;
+        if (st.recoverFrom != 3 || pointFluid(F, a, i)->eosModel != EOS_SW)
+            continue;
+        const int slot = atomicAdd(&a.counters[kCounterAlloc], 1);
+        if (slot >= a.allocCap)
+            continue;
+        AllocMemo<NC> &m = memos[slot];
+        m.P = a.P[i];
+        m.T = a.T[i];
+        m.salinity = st.sal;
+        for (int c = 0; c < NC; ++c)
+            m.z[c] = st.z[c];
+        m.valid = 1;
+        a.allocPoints[slot] = int(i);
+        st.allocSlot = slot;
+    }
+}
+
+// The queued allocation searches, one lane per (point, seed): every lane takes
+// its next task with its own atomic -- a task is a whole preconditioning and
+// refinement solve, so the lanes do not wait for one another -- and writes the
+// seed's outcome into the point's memo.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedAllocSeedKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
+{
+    if (stagedTripped(a))
+        return;
+    const int queued = a.counters[kCounterAlloc];
+    const int64_t points = queued < a.allocCap ? queued : a.allocCap;
+    const int64_t total = points * kAllocSeedCount;
+    const DriverState<NC> *states = static_cast<const DriverState<NC> *>(a.states);
+    AllocMemo<NC> *memos = static_cast<AllocMemo<NC> *>(a.allocMemos);
+    unsigned long long evals = 0;
+    Solver<NC> s;
+    while (true)
+    {
+        const int64_t t = atomicAdd(&a.counters[kCounterAllocCursor], 1);
+        if (t >= total)
+            break;
+        const int64_t slot = t / kAllocSeedCount;
+        const int k = int(t % kAllocSeedCount);
+        const int64_t i = a.allocPoints[slot];
+        if (i < 0 || i >= a.n)
+        {
+            atomicExch(&a.counters[kCounterBound], 17);
+            continue;
+        }
+        const DriverState<NC> &st = states[i];
+        s.setup(pointFluid(F, a, i), st.sal);
+        s.allocationSeedOutcome(a.P[i], a.T[i], st.z, k, memos[slot].seed[k]);
+        evals += s.evals;
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
 // Points whose main path did not end validated: the full solver with its
 // fail-only recoveries, one warp per point.  The lanes run the point in
 // lockstep and split the seeds of every stability test, which cuts the
@@ -951,6 +1046,8 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
         Result<NC> r;
         s.continuation = false;
         const DriverState<NC> &ds = static_cast<const DriverState<NC> *>(a.states)[i];
+        if (a.allocMemos && ds.recoverFrom == 3 && ds.allocSlot >= 0 && ds.allocSlot < a.allocCap)
+            s.allocMemo = static_cast<const AllocMemo<NC> *>(a.allocMemos) + ds.allocSlot;
         if (ds.recoverFrom > 0)
         {
             // the active-set path and the first recoveries already ran (and
@@ -1207,6 +1304,12 @@ size_t stagedScratchBytes(int64_t n, const FluidDev &F)
     const int64_t cap = contCapacity(n);
     add(sizeof(int) * size_t(cap));
     add(sizeof(AnchorOut<NC>) * size_t(cap) * kAnchors);
+    const int64_t acap = allocCapacity(n, F);
+    if (acap > 0)
+    {
+        add(sizeof(AllocMemo<NC>) * size_t(acap));
+        add(sizeof(int) * size_t(acap));
+    }
     return b;
 }
 
@@ -1238,6 +1341,12 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
     a.contCap = contCapacity(n);
     a.cont = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.contCap)));
     a.anchors = take(sizeof(AnchorOut<NC>) * size_t(a.contCap) * kAnchors);
+    a.allocCap = allocCapacity(n, F);
+    if (a.allocCap > 0)
+    {
+        a.allocMemos = take(sizeof(AllocMemo<NC>) * size_t(a.allocCap));
+        a.allocPoints = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.allocCap)));
+    }
     return a;
 }
 
@@ -1319,6 +1428,11 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         stagedRecoverResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, rr);
         if (after("recover round", kMaxRounds + rr + 1))
             return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
+    }
+    if (a.allocCap > 0)
+    {
+        stagedAllocQueueKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a);
+        stagedAllocSeedKernel<NC><<<unsigned(smCount * tune.laneBlocksPerSm), kFlashBlock, 0, st>>>(F, a);
     }
     stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out);
     if (after("full", 0))
