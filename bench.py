@@ -375,10 +375,12 @@ def models_measure(local: int, nmodels: int, cells, seed: int = 21, precision: i
         "component_counts": groups,
         "grouped": {"ms": grouped_ms, "cell_evals_per_s": total / (grouped_ms * 1e-3),
                     "eos_evals_per_cell": evals / max(total, 1), "graph": "one captured CUDA graph",
-                    "kernel_launches": len(groups) * (staged_launches("fp64_staged") + 2) + 2,
+                    "kernel_launches": sum(staged_launches("fp64_staged", sw=any(e == "sw" and c == nc and n > 0
+                                                                                 for c, e, n in specs)) + 2
+                                           for nc in groups),
                     "self_check": {"queue_bound": check_words[0], "spin_guard": check_words[1]}},
         "separate": {"ms": separate_ms, "cell_evals_per_s": total / (separate_ms * 1e-3),
-                     "kernel_launches": sum(1 for _, _, n in specs if n) * staged_launches("fp64_staged")},
+                     "kernel_launches": sum(staged_launches("fp64_staged", sw=e == "sw") for _, e, n in specs if n)},
         "grouped_over_separate": separate_ms / grouped_ms,
         "label_or_status_mismatch_vs_separate": mismatch,
         "autotuner": {"chosen_blocks_per_sm": {str(nc): {"lane": v[0], "warp": v[1]} for nc, v in chosen.items()},
@@ -513,14 +515,17 @@ def run_reference(args):
 FORMS = ("fp64", "fp64_staged", "mixed")
 
 
-def staged_launches(precision_name: str) -> int:
+def staged_launches(precision_name: str, sw: bool = False) -> int:
     """Kernels one batch launches: the plain FP64 form one; the staged forms
-    start, 8 rounds x 8, recovery 1 (5), recovery 2 (3 x 2), the full solver,
-    8 continuation-anchor launches, select and check (+ the polish of the
+    start, 8 rounds x 8, recovery 1 (5), recovery 2 (3 x 2), the recovery
+    kernel (SW: the allocation queue and seed kernels, then the recovery
+    kernel in two passes around the role-permutation kernel), 8
+    continuation-anchor launches, select and check (+ the polish of the
     mixed form)."""
     if precision_name == "fp64":
         return 1
-    return 1 + 8 * 8 + 5 + 3 * 2 + 1 + 8 + 1 + 1 + (1 if precision_name == "mixed" else 0)
+    recovery = 5 if sw else 1
+    return 1 + 8 * 8 + 5 + 3 * 2 + recovery + 8 + 1 + 1 + (1 if precision_name == "mixed" else 0)
 
 
 def form_error(out, ref_out):

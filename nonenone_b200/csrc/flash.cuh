@@ -363,6 +363,38 @@ struct AllocMemo
     }
 };
 
+// The SW role-permutation search (three_phase_flash.hpp:174-205) of one exact
+// input computed ahead of time: for each fixed role permutation k, the
+// nested flash's answer, whether it is usable, its Gibbs energy under those
+// roles and its error.  recover() replays the sequential choice over them.
+template <int NC>
+struct PermOut
+{
+    Result<NC> r;
+    double gibbs;
+    int ok;
+    int err;
+};
+
+template <int NC>
+struct PermMemo
+{
+    double P, T, salinity;
+    double z[NC];
+    int valid;
+    PermOut<NC> perm[6];
+
+    NZ_HD bool matches(double p, double t, double s, const double *zz) const
+    {
+        if (!valid || P != p || T != t || salinity != s)
+            return false;
+        for (int i = 0; i < NC; ++i)
+            if (z[i] != zz[i])
+                return false;
+        return true;
+    }
+};
+
 // ============================================================================
 template <int NC>
 struct Solver
@@ -387,6 +419,11 @@ struct Solver
     StabilityMemo<NC> *stabMemo;   // optional precomputed stability test
     const FlashMemo<NC> *flashMemo;   // optional precomputed top-level flash
     const AllocMemo<NC> *allocMemo;   // optional precomputed SW allocation seeds
+    const PermMemo<NC> *permMemo;     // optional precomputed SW role-permutation search
+    // Staged use: stop recover() where the role-permutation search would
+    // start (reachedPermutations tells), so that it can be run ahead.
+    bool stopAtPermutations;
+    bool reachedPermutations;
     bool mixed;                    // mixed-precision successive substitution in the TPD trials
 
     NZ_HD void setup(const FluidDev *fluid, double s)
@@ -406,6 +443,9 @@ struct Solver
         stabMemo = nullptr;
         flashMemo = nullptr;
         allocMemo = nullptr;
+        permMemo = nullptr;
+        stopAtPermutations = false;
+        reachedPermutations = false;
         mixed = false;
     }
 
@@ -3557,6 +3597,32 @@ struct Solver
         deriveReferenceK(n);
     }
 
+    // One fixed role permutation of recovery 4: the nested flash under roles
+    // swRolePermutation(k) (no permutation search, no continuation), whether
+    // its answer is usable and its Gibbs energy under those roles.  An error
+    // of the nested flash is this solver's error.
+    NZ_HDN void permutedFlash(double P, double T, const double *z, int k, Result<NC> &permuted, bool &ok,
+                              double &g)
+    {
+        int perm[3];
+        swRolePermutation(k, perm);
+        Solver<NC> cand = *this;
+        cand.stabMemo = nullptr;   // stored tests were taken with the default roles
+        cand.allocMemo = nullptr;
+        cand.permMemo = nullptr;
+        cand.roles[0] = perm[0];
+        cand.roles[1] = perm[1];
+        cand.roles[2] = perm[2];
+        cand.permutationSearch = false;
+        cand.continuation = false;
+        cand.template flash<false>(P, T, z, permuted);
+        ok = permuted.converged && cand.err == ERR_NONE;
+        g = ok ? cand.dimensionlessGibbs(P, T, permuted) : 0.0;
+        evals = cand.evals;
+        if (cand.err)
+            fail(cand.err);
+    }
+
     // --------------------------------------------------------------- flash --
     // flash (three_phase_flash.hpp:83-227).  The nested solvers of the
     // role-permutation search and the pressure continuation run with both
@@ -3678,7 +3744,7 @@ struct Solver
         }
         if (err)
             return;
-        if (sw())
+        if (from <= 3 && sw())
         {
             // recovery 3 (SW only): exact-mass allocation basin search
             Result<NC> allocated;
@@ -3699,9 +3765,16 @@ struct Solver
                 }
             }
         }
-        if (TopLevel && sw() && permutationSearch)
+        if (TopLevel && sw() && permutationSearch && from <= 4)
         {
             // recovery 4 (SW only): the other fixed role permutations (three_phase_flash.hpp:174-205)
+            if (stopAtPermutations)
+            {
+                reachedPermutations = true;
+                return;
+            }
+            const bool replay = permMemo && roles[0] == OIL && roles[1] == GAS && roles[2] == WATER &&
+                                permMemo->matches(P, T, salinity, z);
             Result<NC> bestPermuted, permuted;
             bestPermuted.init();
             double bestG = nzInf();
@@ -3712,22 +3785,25 @@ struct Solver
                 swRolePermutation(k, perm);
                 if (perm[0] == roles[0] && perm[1] == roles[1] && perm[2] == roles[2])
                     continue;
-                Solver<NC> cand = *this;
-                cand.stabMemo = nullptr;   // stored tests were taken with the default roles
-                cand.allocMemo = nullptr;
-                cand.roles[0] = perm[0];
-                cand.roles[1] = perm[1];
-                cand.roles[2] = perm[2];
-                cand.permutationSearch = false;
-                cand.continuation = false;
-                cand.template flash<false>(P, T, z, permuted);
-                const bool ok = permuted.converged && cand.err == ERR_NONE;
-                const double g = ok ? cand.dimensionlessGibbs(P, T, permuted) : 0.0;
-                evals = cand.evals;
-                if (cand.err)
+                bool ok;
+                double g;
+                if (replay)
                 {
-                    fail(cand.err);
-                    return;
+                    const PermOut<NC> &o = permMemo->perm[k];
+                    if (o.err)
+                    {
+                        fail(o.err);
+                        return;
+                    }
+                    ok = o.ok != 0;
+                    g = o.gibbs;
+                    permuted = o.r;
+                }
+                else
+                {
+                    permutedFlash(P, T, z, k, permuted, ok, g);
+                    if (err)
+                        return;
                 }
                 if (!ok)
                     continue;
@@ -3761,13 +3837,19 @@ struct Solver
     // holds the continued result) or CONT_ERROR (err is set).  Anchors are
     // independent of one another, so they may run in any order or in parallel;
     // the fallback's answer is that of the first anchor that is not CONT_NONE.
-    NZ_HDN int continuationAnchor(double P, double T, const double *z, int a, Result<NC> &out)
+    // Pressure ratio of anchor a (restricted.inc:554-627).
+    NZ_HD static double continuationRatio(int a)
     {
         const double ratios[8] = {0.95, 1.05, 0.90, 1.10, 0.80, 1.25, 0.65, 1.50};
-        const double anchorP = P * ratios[a];
+        return ratios[a];
+    }
+
+    NZ_HDN int continuationAnchor(double P, double T, const double *z, int a, Result<NC> &out)
+    {
+        const double anchorP = P * continuationRatio(a);
         if (!(anchorP > 0.0) || !isfinite(anchorP))
             return CONT_NONE;
-        Result<NC> anchor, current;
+        Result<NC> anchor;
         {
             Solver<NC> nested = *this;
             nested.permutationSearch = false;
@@ -3780,6 +3862,16 @@ struct Solver
                 return CONT_ERROR;
             }
         }
+        return continuationPath(P, T, z, a, anchor, out);
+    }
+
+    // The log-pressure path of anchor a from its converged anchor flash
+    // `anchor` (taken at P * continuationRatio(a)) to P.
+    NZ_HDN int continuationPath(double P, double T, const double *z, int a, const Result<NC> &anchor,
+                                Result<NC> &out)
+    {
+        const double anchorP = P * continuationRatio(a);
+        Result<NC> current;
         if (!anchor.converged)
             return CONT_NONE;
         numericalSwRoleResult(anchor, out);

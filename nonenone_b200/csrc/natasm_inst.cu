@@ -46,7 +46,7 @@ int natLaunchAssembly(int op, const NatLaunch &a, cudaStream_t st)
         break;
     case NAT_JACOBIAN:
     {
-        // directions per lane: 1 = natJacobianKernel, else natJacobianKernelN
+        // directions per lane: 1 = natJacobianKernel, 2-5 natJacobianKernelN
         static const int kdir = [] {
             const char *v = std::getenv("NZ_JACOBIAN_K");
             return v ? std::atoi(v) : 5;
@@ -60,7 +60,10 @@ int natLaunchAssembly(int op, const NatLaunch &a, cudaStream_t st)
                                                               a.residual, a.flag);
             break;
         }
-        const int rc = kdir == 2 ? launchJacobianN<NC, 2>(a, st) : launchJacobianN<NC, 5>(a, st);
+        const int rc = kdir == 2   ? launchJacobianN<NC, 2>(a, st)
+                       : kdir == 3 ? launchJacobianN<NC, 3>(a, st)
+                       : kdir == 4 ? launchJacobianN<NC, 4>(a, st)
+                                   : launchJacobianN<NC, 5>(a, st);
         if (rc != NZ_OK)
             return rc;
         break;

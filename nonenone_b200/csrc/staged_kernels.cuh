@@ -84,6 +84,10 @@ struct StagedArgs
     void *allocMemos;
     int *allocPoints;
     int64_t allocCap;
+    // the role-permutation searches of the same points (PermMemo<NC>[allocCap],
+    // indexed by the allocation slot) and the slots queued for them
+    void *permMemos;
+    int *permSlots;
 };
 
 // The fluid point i is flashed with, and its salinity.
@@ -111,6 +115,7 @@ constexpr int kCounterThreeCursor = kCounterFull + 7;  // refill cursor of the t
 constexpr int kCounterThreeLong = kCounterFull + 8;    // solves handed to the warp kernel
 constexpr int kCounterAlloc = kCounterFull + 9;        // points queued for the lane allocation search
 constexpr int kCounterAllocCursor = kCounterFull + 10; // its (point, seed) task cursor
+constexpr int kCounterPerm = kCounterFull + 11;        // points queued for the warp permutation search
 // Steps a lane of the three-phase kernel gives one solve before handing it to
 // the warp kernel.  Most solves end within ~40 steps; the few long ones are
 // long because their robust Rachford-Rice solves fail start after start,
@@ -1011,6 +1016,68 @@ stagedAllocSeedKernel(const __grid_constant__ FluidDev F, const __grid_constant_
     warpAddEvals(a.evalCounter, evals);
 }
 
+// The role-permutation searches of the points the first recovery pass
+// stopped: one warp per (point, permutation), each the nested flash under
+// that permutation's roles (Solver::permutedFlash), written to the point's
+// memo for the second pass.
+template <int NC>
+__global__ void __launch_bounds__(kFlashBlock)
+stagedPermKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
+{
+    if (stagedTripped(a))
+        return;
+    const int queued = a.counters[kCounterPerm];
+    const int64_t count = queued < a.allocCap ? queued : a.allocCap;
+    const int lane = threadIdx.x & 31;
+    const int64_t warpId = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    PermMemo<NC> *memos = static_cast<PermMemo<NC> *>(a.permMemos);
+    const DriverState<NC> *states = static_cast<const DriverState<NC> *>(a.states);
+    unsigned long long evals = 0;
+    for (int64_t t = warpId; t < count * 6; t += nwarps)
+    {
+        const int slot = a.permSlots[t / 6];
+        const int k = int(t % 6);
+        int perm[3];
+        swRolePermutation(k, perm);
+        if (perm[0] == OIL && perm[1] == GAS && perm[2] == WATER)
+            continue;   // the default roles: not part of the search
+        if (slot < 0 || slot >= a.allocCap)
+        {
+            if (lane == 0)
+                atomicExch(&a.counters[kCounterBound], 19);
+            continue;
+        }
+        const int64_t i = a.allocPoints[slot];
+        if (i < 0 || i >= a.n)
+        {
+            if (lane == 0)
+                atomicExch(&a.counters[kCounterBound], 20);
+            continue;
+        }
+        const DriverState<NC> &st = states[i];
+        Solver<NC> s;
+        s.setup(pointFluid(F, a, i), st.sal);
+        s.lane = lane;
+        s.width = 32;
+        Result<NC> r;
+        bool ok = false;
+        double g = 0.0;
+        s.permutedFlash(a.P[i], a.T[i], st.z, k, r, ok, g);
+        __syncwarp();
+        if (lane == 0)
+        {
+            PermOut<NC> &o = memos[slot].perm[k];
+            o.r = r;
+            o.gibbs = g;
+            o.ok = ok ? 1 : 0;
+            o.err = s.err;
+            evals += s.evals;
+        }
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
 // Points whose main path did not end validated: the full solver with its
 // fail-only recoveries, one warp per point.  The lanes run the point in
 // lockstep and split the seeds of every stability test, which cuts the
@@ -1018,7 +1085,7 @@ stagedAllocSeedKernel(const __grid_constant__ FluidDev F, const __grid_constant_
 template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
 stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a,
-                 const __grid_constant__ nz_flash_out out)
+                 const __grid_constant__ nz_flash_out out, int phase)
 {
     if (stagedTripped(a))
         return;
@@ -1045,9 +1112,20 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
             zi[c] = a.z[c * a.n + i];
         Result<NC> r;
         s.continuation = false;
-        const DriverState<NC> &ds = static_cast<const DriverState<NC> *>(a.states)[i];
-        if (a.allocMemos && ds.recoverFrom == 3 && ds.allocSlot >= 0 && ds.allocSlot < a.allocCap)
+        DriverState<NC> &ds = static_cast<DriverState<NC> *>(a.states)[i];
+        // phase 0: one pass; phase 1: every point, those with memo slots
+        // stopping where the role-permutation search starts; phase 2: the
+        // stopped points, the search replayed from its memo
+        const bool slotted = a.allocMemos && ds.allocSlot >= 0 && ds.allocSlot < a.allocCap;
+        if (phase == 2 && !(ds.recoverFrom == 4 && slotted))
+            continue;
+        if (slotted && ds.recoverFrom == 3)
+        {
             s.allocMemo = static_cast<const AllocMemo<NC> *>(a.allocMemos) + ds.allocSlot;
+            s.stopAtPermutations = phase == 1 && a.permMemos != nullptr;
+        }
+        if (phase == 2)
+            s.permMemo = static_cast<const PermMemo<NC> *>(a.permMemos) + ds.allocSlot;
         if (ds.recoverFrom > 0)
         {
             // the active-set path and the first recoveries already ran (and
@@ -1057,6 +1135,29 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
         }
         else
             s.template flash<true>(a.P[i], a.T[i], zi, r);
+        if (s.reachedPermutations)
+        {
+            // hand the point to the permutation kernel; phase 2 finishes it
+            __syncwarp();
+            if (lane == 0)
+            {
+                PermMemo<NC> &m = static_cast<PermMemo<NC> *>(a.permMemos)[ds.allocSlot];
+                m.P = a.P[i];
+                m.T = a.T[i];
+                m.salinity = s.salinity;
+                for (int c = 0; c < NC; ++c)
+                    m.z[c] = ds.z[c];
+                m.valid = 1;
+                ds.recoverFrom = 4;
+                const int q = atomicAdd(&a.counters[kCounterPerm], 1);
+                if (q < a.allocCap)
+                    a.permSlots[q] = ds.allocSlot;
+                else
+                    atomicExch(&a.counters[kCounterBound], 18);
+                evals += s.evals;
+            }
+            continue;
+        }
         if (s.err == ERR_NONE && !r.converged)
         {
             // Every recovery but the pressure continuation has failed.  Queue the
@@ -1309,6 +1410,8 @@ size_t stagedScratchBytes(int64_t n, const FluidDev &F)
     {
         add(sizeof(AllocMemo<NC>) * size_t(acap));
         add(sizeof(int) * size_t(acap));
+        add(sizeof(PermMemo<NC>) * size_t(acap));
+        add(sizeof(int) * size_t(acap));
     }
     return b;
 }
@@ -1346,6 +1449,8 @@ StagedArgs stagedCarve(void *scratch, int64_t n, const FluidDev &F)
     {
         a.allocMemos = take(sizeof(AllocMemo<NC>) * size_t(a.allocCap));
         a.allocPoints = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.allocCap)));
+        a.permMemos = take(sizeof(PermMemo<NC>) * size_t(a.allocCap));
+        a.permSlots = reinterpret_cast<int *>(take(sizeof(int) * size_t(a.allocCap)));
     }
     return a;
 }
@@ -1433,8 +1538,12 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     {
         stagedAllocQueueKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a);
         stagedAllocSeedKernel<NC><<<unsigned(smCount * tune.laneBlocksPerSm), kFlashBlock, 0, st>>>(F, a);
+        stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out, 1);
+        stagedPermKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a);
+        stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out, 2);
     }
-    stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out);
+    else
+        stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out, 0);
     if (after("full", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the full solver");
     // one launch per anchor, each for the points no earlier anchor decided:

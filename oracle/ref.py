@@ -187,6 +187,14 @@ class Natural:
             raise RuntimeError(f"PTz flash failed at cell {rc - 1}")
         return primary, ps
 
+    def update_cell_seconds(self):
+        """Seconds each cell's updatePhaseState took in the last update_state."""
+        out = np.zeros(self.grid.ncell)
+        L = lib()
+        L.nzref_natural_update_cell_seconds.restype = C.c_int64
+        L.nzref_natural_update_cell_seconds(self.h, _p(out))
+        return out
+
     def set_threads(self, threads: int):
         """Worker threads of the cell loops (one kernel each); the results do
         not depend on the count."""

@@ -28,6 +28,7 @@
 #include "../include/nonenone_b200.h"
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -361,6 +362,8 @@ struct NaturalBase
     virtual int setHistory(const double *primary, const double *ps) = 0;
     virtual int updateState(double *primary, double *ps, nz_report *report) = 0;
     virtual void setThreads(int n) = 0;
+    // Seconds each cell's updatePhaseState took in the last updateState.
+    std::vector<double> cellSeconds;
     virtual int residual(const double *primary, const double *ps, double *F) = 0;
     virtual int jacobian(const double *primary, const double *ps, double *vals) = 0;
     virtual int pattern(int64_t *rowPtr, int64_t *colIdx, int64_t *nnzb) = 0;
@@ -591,6 +594,7 @@ struct Natural final : NaturalBase
 
     int updateState(double *primary, double *ps, nz_report *report) override
     {
+        cellSeconds.assign(static_cast<std::size_t>(ncell), 0.0);
         std::vector<PrimaryArray> newPrimary(ncell);
         std::vector<PhaseStateData<I>> newPs(ncell);
         nz_report r{};
@@ -604,6 +608,7 @@ struct Natural final : NaturalBase
             {
                 auto a = readPrimary(primary, c);
                 auto s = readPs(ps, c);
+                const auto t0 = std::chrono::steady_clock::now();
                 eq.sanitizePrimaryBeforeFlash(a, false);
                 PhaseUpdateResult u;
                 try
@@ -614,6 +619,7 @@ struct Natural final : NaturalBase
                 {
                     u.status = PhaseUpdateStatus::RecoverableThermodynamicFailure;
                 }
+                cellSeconds[c] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
                 results[c] = u;
                 newPrimary[c] = a;
                 newPs[c] = s;
@@ -969,6 +975,14 @@ int nzref_jacobian(void *h, const double *primary, const double *ps, double *val
 void nzref_natural_set_threads(void *h, int threads)
 {
     static_cast<NaturalBase *>(h)->setThreads(threads);
+}
+// Per-cell seconds of the last update (out: ncell doubles); returns the count.
+int64_t nzref_natural_update_cell_seconds(void *h, double *out)
+{
+    const auto &v = static_cast<NaturalBase *>(h)->cellSeconds;
+    for (std::size_t c = 0; c < v.size(); ++c)
+        out[c] = v[c];
+    return int64_t(v.size());
 }
 int nzref_natural_pattern(void *h, int64_t *rowPtr, int64_t *colIdx, int64_t *nnzb)
 {

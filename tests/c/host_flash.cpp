@@ -10,7 +10,9 @@
 // search precomputed seed by seed into an AllocMemo (the staged kernels'
 // lane form) -- and prints the number of points whose answers differ in any
 // bit, and how many points read their memo (those whose answer changes when
-// every seed of the memo is made inadmissible).
+// every seed of the memo is made inadmissible); likewise the role-permutation
+// search stopped where it starts, run ahead into a PermMemo and replayed
+// (and how many points reached it).
 #include "nonenone_b200.h"
 #include "fluid_dev.cuh"
 #include "staged.cuh"
@@ -72,7 +74,7 @@ static int run(const std::string &dir, const FluidDev &F, bool memoMode)
     }
     std::vector<uint8_t> presence(n), status(n);
     std::vector<double> beta(3 * n);
-    long differ = 0, replayed = 0;
+    long differ = 0, replayed = 0, permuted = 0;
     for (size_t i = 0; i < n; ++i)
     {
         double zi[NC];
@@ -118,6 +120,44 @@ static int run(const std::string &dir, const FluidDev &F, bool memoMode)
         m.template flash<true>(P[i], T[i], zi, rm);
         if (m.err != s.err || !sameResult(r, rm))
             ++differ;
+        // the role-permutation search the same way: stop where it starts,
+        // run every permutation ahead into a PermMemo, then replay it
+        Solver<NC> stop;
+        stop.setup(&F, s0);
+        stop.allocMemo = &memo;
+        stop.stopAtPermutations = true;
+        Result<NC> rs;
+        stop.template flash<true>(P[i], T[i], zi, rs);
+        if (stop.reachedPermutations)
+        {
+            ++permuted;
+            PermMemo<NC> pm{};
+            pm.P = P[i];
+            pm.T = T[i];
+            pm.salinity = s0;
+            for (int c = 0; c < NC; ++c)
+                pm.z[c] = zn[c];
+            pm.valid = 1;
+            for (int k = 0; k < 6; ++k)
+            {
+                Solver<NC> w;
+                w.setup(&F, s0);
+                bool ok = false;
+                double g = 0.0;
+                w.permutedFlash(P[i], T[i], zn, k, pm.perm[k].r, ok, g);
+                pm.perm[k].ok = ok ? 1 : 0;
+                pm.perm[k].gibbs = g;
+                pm.perm[k].err = w.err;
+            }
+            Solver<NC> rp;
+            rp.setup(&F, s0);
+            rp.allocMemo = &memo;
+            rp.permMemo = &pm;
+            Result<NC> rr;
+            rp.template flash<true>(P[i], T[i], zi, rr);
+            if (rp.err != s.err || !sameResult(r, rr))
+                ++differ;
+        }
         // the points whose search read the memo: a memo in which no seed is
         // admissible changes exactly their answers
         AllocMemo<NC> empty = memo;
@@ -138,7 +178,7 @@ static int run(const std::string &dir, const FluidDev &F, bool memoMode)
     writeBin(dir, "status.bin", status);
     writeBin(dir, "beta.bin", beta);
     if (memoMode)
-        std::printf("points %zu differ %ld memos %ld\n", n, differ, replayed);
+        std::printf("points %zu differ %ld memos %ld permuted %ld\n", n, differ, replayed, permuted);
     else
         std::printf("points %zu\n", n);
     return 0;

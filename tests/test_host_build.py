@@ -6,7 +6,7 @@ phase fractions), where no FMA contraction or device libm rounding intervenes.
 And the SW allocation search precomputed seed by seed into an AllocMemo (the
 staged kernels' lane form) must give every point exactly the answer of the
 search run in place, with the memo demonstrably read by the points that reach
-the search.
+the search; likewise the role-permutation search run ahead into a PermMemo.
 """
 import ctypes as C
 import os
@@ -85,5 +85,7 @@ def test_allocation_memo_replays_the_search(host_flash, tmp_path):
     stats = dict(zip(out[0::2], (int(v) for v in out[1::2])))
     assert stats["points"] == n
     assert stats["differ"] == 0
-    # the fixture's SW mixture sends a few percent of its points to the search
+    # the fixture's SW mixture sends a few percent of its points to the search,
+    # and at least one of them on to the role-permutation search
     assert stats["memos"] >= 5, stats
+    assert stats["permuted"] >= 1, stats
