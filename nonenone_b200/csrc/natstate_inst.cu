@@ -61,9 +61,23 @@ int natLaunch(int op, const NatLaunch &a, cudaStream_t st)
         break;
     }
     case NAT_INIT:
-        natInitKernel<NC><<<warpGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
-                                                         a.firstFailure, width);
+    {
+        // with a work space: every cell's flash through the batched flash
+        // first, the per-cell kernel then assigning from its memo
+        FlashMemo<NC> *memos = nullptr;
+        int initWidth = width;
+        if (a.flashScratch)
+        {
+            const int rc = natInitFlash<NC>(a.F, a.K, n, a.initP, a.initZ, a.flashScratch, smCount, st, &memos);
+            if (rc != NZ_OK)
+                return rc;
+            initWidth = 1;
+        }
+        const unsigned initGrid = unsigned((n * initWidth + kNatBlock - 1) / kNatBlock);
+        natInitKernel<NC><<<initGrid, kNatBlock, 0, st>>>(a.F, a.K, n, a.initP, a.initZ, a.newPrimary, a.newPs,
+                                                         a.firstFailure, initWidth, memos);
         break;
+    }
     default:
         return setError(NZ_ERR_ARGUMENT, "natLaunch: unknown operation %d", op);
     }
@@ -89,7 +103,14 @@ int *natReflashCountNc(void *scratch, int64_t n, const FluidDev &F)
     return natStagedCarve<NC>(scratch, n, F).count;
 }
 
+template <int NC>
+size_t natInitBytesNc(int64_t n, const FluidDev &F)
+{
+    return natInitBytes<NC>(n, F);
+}
+
 template int natLaunch<NZ_INST_NC>(int, const NatLaunch &, cudaStream_t);
+template size_t natInitBytesNc<NZ_INST_NC>(int64_t, const FluidDev &);
 template size_t natStagedBytesNc<NZ_INST_NC>(int64_t, const FluidDev &);
 template size_t natReflashBytesNc<NZ_INST_NC>(int64_t, const FluidDev &);
 template int *natReflashCountNc<NZ_INST_NC>(void *, int64_t, const FluidDev &);

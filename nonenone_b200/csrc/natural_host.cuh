@@ -36,7 +36,8 @@ struct NatLaunch
     const double *initP;   // NAT_INIT: P[ncell], z[ncell][nc]
     const double *initZ;
     void *stagedScratch;   // staged update: natStagedBytesNc<NC> bytes, or null for the per-cell update
-    void *flashScratch;    // NAT_UPDATE_REFLASH: natReflashBytesNc<NC>(reflashCount) bytes
+    void *flashScratch;    // NAT_UPDATE_REFLASH: natReflashBytesNc<NC>(reflashCount) bytes;
+                           // NAT_INIT: natInitBytesNc<NC>(ncell) bytes, or null for the per-cell flash
     int reflashCount;
 };
 
@@ -51,4 +52,7 @@ template <int NC>
 size_t natReflashBytesNc(int64_t n, const FluidDev &F);
 template <int NC>
 int *natReflashCountNc(void *scratch, int64_t n, const FluidDev &F);
+// Work space of the batched P-T-z initialisation of n cells.
+template <int NC>
+size_t natInitBytesNc(int64_t n, const FluidDev &F);
 } // namespace nz

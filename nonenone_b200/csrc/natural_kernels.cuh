@@ -284,13 +284,15 @@ NZ_HD bool cellUpdateHead(const FluidDev &F, const NatConst &K, const double *pr
 // flash does not converge (the reference throws).
 template <int NC>
 NZ_HD bool cellInitPtz(const FluidDev &F, const NatConst &K, const double *P, const double *z, int64_t c,
-                       double *primary, double *ps, int lane = 0, int width = 1)
+                       double *primary, double *ps, int lane = 0, int width = 1,
+                       const FlashMemo<NC> *memo = nullptr)
 {
     using L = Layout<NC>;
     Equilibrium<NC> eq;
     eq.s.setup(&F, F.salinity);
     eq.s.lane = lane;
     eq.s.width = width;
+    eq.s.flashMemo = memo;   // the batched flash's answer for this cell's input, if given
     eq.K = &K;
     Result<NC> r;
     eq.s.template flash<true>(P[c], K.temperature, z + c * NC, r);
@@ -557,13 +559,14 @@ template <int NC>
 __global__ void __launch_bounds__(kNatBlock) natInitKernel(const __grid_constant__ FluidDev F,
                                                            const __grid_constant__ NatConst K, int64_t ncell,
                                                            const double *P, const double *z, double *primary,
-                                                           double *ps, unsigned long long *firstFailure, int width)
+                                                           double *ps, unsigned long long *firstFailure, int width,
+                                                           const FlashMemo<NC> *memos)
 {
     const int lane = width == 32 ? int(threadIdx.x & 31) : 0;
     const int64_t c = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / width;
     if (c >= ncell)
         return;
-    if (!cellInitPtz<NC>(F, K, P, z, c, primary, ps, lane, width) && lane == 0)
+    if (!cellInitPtz<NC>(F, K, P, z, c, primary, ps, lane, width, memos ? memos + c : nullptr) && lane == 0)
         atomicMin(firstFailure, (unsigned long long)c);
 }
 #endif

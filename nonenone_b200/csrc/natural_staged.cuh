@@ -386,6 +386,115 @@ int natReflash(const FluidDev &F, int64_t ncell, void *scratch, void *flashScrat
     return e == cudaSuccess ? NZ_OK : cudaFail(e, "Natural reflash launch");
 }
 
+// P-T-z initialisation through the batched flash: every cell's input
+// (P[c], the case temperature, z[c][:]) flashed by the staged kernels, the
+// answers kept as per-cell flash memos for natInitKernel.
+template <int NC>
+size_t natInitBytes(int64_t n, const FluidDev &F)
+{
+    size_t b = 0;
+    auto add = [&](size_t bytes) { b += (bytes + 255) & ~size_t(255); };
+    add(stagedScratchBytes<NC>(n, F));
+    add(sizeof(FlashMemo<NC>) * size_t(n));
+    add(sizeof(double) * size_t(n) * (2 + NC));               // P, T, z
+    add(size_t(n) * 2);                                        // status, presence
+    add(sizeof(int32_t) * size_t(n));                          // iterations
+    add(sizeof(double) * size_t(n) * (4 * 3 + 3 * NC + 2 * NC));
+    add(sizeof(unsigned long long));                           // evaluation count
+    return b;
+}
+
+template <int NC>
+__global__ void natInitGatherKernel(int64_t n, const __grid_constant__ NatConst K, const double *Pin,
+                                    const double *zin, double *P, double *T, double *z)
+{
+    for (int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < n; c += int64_t(gridDim.x) * blockDim.x)
+    {
+        P[c] = Pin[c];
+        T[c] = K.temperature;
+        for (int i = 0; i < NC; ++i)
+            z[size_t(i) * n + c] = zin[c * NC + i];
+    }
+}
+
+template <int NC>
+__global__ void natInitMemoKernel(int64_t n, const __grid_constant__ NatConst K, const double *Pin,
+                                  const double *zin, const __grid_constant__ nz_flash_out out, FlashMemo<NC> *memos)
+{
+    for (int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < n; c += int64_t(gridDim.x) * blockDim.x)
+    {
+        FlashMemo<NC> &f = memos[c];
+        f.P = Pin[c];
+        f.T = K.temperature;
+        for (int i = 0; i < NC; ++i)
+            f.z[i] = zin[c * NC + i];
+        const uint8_t status = out.status[c];
+        Result<NC> &r = f.r;
+        r.converged = status == NZ_FLASH_CONVERGED;
+        r.iterations = out.iterations[c];
+        r.presence = out.presence[c];
+        for (int p = 0; p < 3; ++p)
+        {
+            r.beta[p] = out.beta[size_t(p) * n + c];
+            r.sat[p] = out.saturation[size_t(p) * n + c];
+            r.Z[p] = out.compressibility[size_t(p) * n + c];
+            r.rho[p] = out.molar_density[size_t(p) * n + c];
+            for (int i = 0; i < NC; ++i)
+                r.x[p][i] = out.composition[(size_t(p) * NC + i) * n + c];
+        }
+        for (int i = 0; i < NC; ++i)
+        {
+            r.Kg[i] = out.k_gas_oil[size_t(i) * n + c];
+            r.Kw[i] = out.k_water_oil[size_t(i) * n + c];
+        }
+        f.err = status > NZ_FLASH_FAILED ? int(status) : ERR_NONE;
+        f.valid = 1;
+    }
+}
+
+// The batched flash of every cell into the memos carved from `scratch`
+// (natInitBytes<NC>(n) bytes); returns the memos' address through `memos`.
+template <int NC>
+int natInitFlash(const FluidDev &F, const NatConst &K, int64_t n, const double *Pin, const double *zin,
+                 void *scratch, int smCount, cudaStream_t st, FlashMemo<NC> **memos)
+{
+    char *p = static_cast<char *>(scratch);
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) & ~size_t(255);
+        return r;
+    };
+    void *flashScratch = take(stagedScratchBytes<NC>(n, F));
+    FlashMemo<NC> *m = reinterpret_cast<FlashMemo<NC> *>(take(sizeof(FlashMemo<NC>) * size_t(n)));
+    double *P = reinterpret_cast<double *>(take(sizeof(double) * size_t(n) * (2 + NC)));
+    double *T = P + n;
+    double *z = T + n;
+    nz_flash_out out{};
+    out.status = reinterpret_cast<uint8_t *>(take(size_t(n) * 2));
+    out.presence = out.status + n;
+    out.iterations = reinterpret_cast<int32_t *>(take(sizeof(int32_t) * size_t(n)));
+    double *d = reinterpret_cast<double *>(take(sizeof(double) * size_t(n) * (4 * 3 + 3 * NC + 2 * NC)));
+    out.beta = d;
+    out.saturation = d + 3 * size_t(n);
+    out.compressibility = d + 6 * size_t(n);
+    out.molar_density = d + 9 * size_t(n);
+    out.composition = d + 12 * size_t(n);
+    out.k_gas_oil = out.composition + 3 * NC * size_t(n);
+    out.k_water_oil = out.k_gas_oil + NC * size_t(n);
+    unsigned long long *evals = reinterpret_cast<unsigned long long *>(take(sizeof(unsigned long long)));
+    const int64_t blocks = (n + 255) / 256;
+    const unsigned grid = unsigned(blocks < int64_t(smCount) * 8 ? blocks : int64_t(smCount) * 8);
+    natInitGatherKernel<NC><<<grid, 256, 0, st>>>(n, K, Pin, zin, P, T, z);
+    cudaMemsetAsync(evals, 0, sizeof(unsigned long long), st);
+    int rc = stagedLaunchExt<NC>(F, flashScratch, n, P, T, z, nullptr, out, evals, smCount, st, false);
+    if (rc != 0)
+        return rc;
+    natInitMemoKernel<NC><<<grid, 256, 0, st>>>(n, K, Pin, zin, out, m);
+    *memos = m;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? NZ_OK : cudaFail(e, "Natural P-T-z initialisation flash");
+}
+
 // Prefix, trials, combine and select on `st`; afterwards the host reads the
 // reflash count, runs natReflash, and the update kernel runs with the memos.
 template <int NC>

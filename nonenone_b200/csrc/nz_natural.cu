@@ -35,6 +35,7 @@ using nz::NAT_UPDATE_REFLASH;
 using nz::natLaunch;
 using nz::natStagedBytesNc;
 using nz::natReflashBytesNc;
+using nz::natInitBytesNc;
 using nz::natReflashCountNc;
 using nz::NatConst;
 using nz::NatGeom;
@@ -142,6 +143,19 @@ size_t natStagedBytesFor(int nc, int64_t n, const FluidDev &F)
     case 5: return natStagedBytesNc<5>(n, F);
     case 6: return natStagedBytesNc<6>(n, F);
     case 8: return natStagedBytesNc<8>(n, F);
+    default: return 0;
+    }
+}
+
+size_t natInitBytesFor(int nc, int64_t n, const FluidDev &F)
+{
+    switch (nc)
+    {
+    case 3: return natInitBytesNc<3>(n, F);
+    case 4: return natInitBytesNc<4>(n, F);
+    case 5: return natInitBytesNc<5>(n, F);
+    case 6: return natInitBytesNc<6>(n, F);
+    case 8: return natInitBytesNc<8>(n, F);
     default: return 0;
     }
 }
@@ -492,9 +506,26 @@ int nz_natural_init_ptz(nz_natural *nat, const double *P, const double *z, doubl
     a.newPrimary = nat->newPrimary;
     a.newPs = nat->newPs;
     a.firstFailure = nat->firstFailure;
+    // every cell's flash through the batched flash (its work space held for
+    // this call only), unless the per-cell update form was asked for
+    void *initScratch = nullptr;
+    if (nat->updateMode != NZ_UPDATE_PER_CELL)
+    {
+        e = cudaMalloc(&initScratch, natInitBytesFor(nat->nc, nat->ncell, nat->ctx->fluid));
+        if (e != cudaSuccess)
+            return cudaFail(e, "nz_natural_init_ptz: work space");
+        a.flashScratch = initScratch;
+    }
     int rc = natDispatch(nat->nc, NAT_INIT, a, st);
     if (rc != NZ_OK)
+    {
+        if (initScratch)
+        {
+            cudaStreamSynchronize(st);
+            cudaFree(initScratch);
+        }
         return rc;
+    }
     const int64_t total = nat->ncell * std::max(nat->B, nat->NPS);
     const unsigned grid = unsigned(std::min<int64_t>((total + 255) / 256, 4 * 148));
     natCommitKernel<<<grid, 256, 0, st>>>(nat->ncell, nat->B, nat->NPS, nat->firstFailure, nat->newPrimary,
@@ -506,6 +537,8 @@ int nz_natural_init_ptz(nz_natural *nat, const double *P, const double *z, doubl
                             cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(st);
+    if (initScratch)
+        cudaFree(initScratch);
     if (e != cudaSuccess)
         return cudaFail(e, "nz_natural_init_ptz");
     first = static_cast<unsigned long long>(nat->pinned->report.first_failure_cell);

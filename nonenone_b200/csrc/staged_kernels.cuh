@@ -978,10 +978,10 @@ stagedAllocQueueKernel(const __grid_constant__ FluidDev F, const __grid_constant
     }
 }
 
-// The queued allocation searches, one lane per (point, seed): every lane takes
-// its next task with its own atomic -- a task is a whole preconditioning and
-// refinement solve, so the lanes do not wait for one another -- and writes the
-// seed's outcome into the point's memo.
+// The queued allocation searches, one lane per (seed, point) task, tasks in
+// seed-major order: every lane takes its next task with its own atomic -- a
+// task is a whole preconditioning and refinement solve, so the lanes do not
+// wait for one another -- and writes the seed's outcome into the point's memo.
 template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
 stagedAllocSeedKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
@@ -1000,8 +1000,10 @@ stagedAllocSeedKernel(const __grid_constant__ FluidDev F, const __grid_constant_
         const int64_t t = atomicAdd(&a.counters[kCounterAllocCursor], 1);
         if (t >= total)
             break;
-        const int64_t slot = t / kAllocSeedCount;
-        const int k = int(t % kAllocSeedCount);
+        // seed-major: consecutive lanes take the same seed of different
+        // points, so a warp's lanes start in the same seed builder
+        const int k = int(t / points);
+        const int64_t slot = t % points;
         const int64_t i = a.allocPoints[slot];
         if (i < 0 || i >= a.n)
         {
