@@ -453,6 +453,25 @@ def cpa_assembly_measure(local, shape, hbm_peak, relperm, timed, block=(20, 20))
                               "achieved": jac_bytes / (jac_ms * 1e-3) / 1e9, "unit": "GB/s", "peak": hbm_peak,
                               "frac": (jac_bytes / (jac_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None},
     }
+    # the reference's residual + Jacobian loops on all host threads, over the
+    # flashed column (its own grid, the same accepted state), per cell
+    try:
+        from oracle import ref
+        threads = os.cpu_count() or 1
+        o = ref.Natural(fluid, sub, 864.0, temperature, relperm)
+        o.set_threads(threads)
+        pb, sb = p_blk.cpu().numpy(), s_blk.cpu().numpy()
+        o.set_history(pb, sb)
+        tc = time.perf_counter()
+        o.residual(pb, sb)
+        o.jacobian(pb, sb)
+        cpu_s = time.perf_counter() - tc
+        out["cpu_reference"] = {"threads": threads, "cells": sub.ncell, "newton_assembly_ms": cpu_s * 1e3,
+                                "cell_evals_per_s": sub.ncell / cpu_s, "kind": "reference",
+                                "what": f"the reference's residual and Jacobian loops (oracle/_ref) on the "
+                                        f"{bx}x{by}x{nz} column at its accepted state"}
+    except Exception as ex:   # the compiled reference is test infrastructure; report, do not fail
+        out["cpu_reference"] = {"error": str(ex)}
     del nat, vals, host_vals
     return out
 

@@ -372,7 +372,10 @@ int nz_natural_pattern(nz_natural* nat, int64_t* row_ptr, int64_t* col_idx,
  * with one (P, z) per cell.  P[ncell], z[ncell][nc] (cell-major), primary and
  * phase_state outputs, all device pointers.  Returns NZ_RECOVERABLE, with
  * *first_failure = the lowest failing cell, when a flash does not converge
- * (the reference throws); nothing is written then. */
+ * (the reference throws); nothing is written then.  Unless the per-cell
+ * update mode is set (nz_natural_set_update_mode), every cell's flash runs
+ * through the batched staged flash first, in a work space allocated for the
+ * call (about 2.5 KB per cell for nc = 3). */
 int nz_natural_init_ptz(nz_natural* nat, const double* P, const double* z,
                         double* primary, double* phase_state,
                         int64_t* first_failure, void* stream);
