@@ -285,8 +285,9 @@ int nz_models_destroy(nz_models* m);
 int nz_models_flash(nz_models* m, const nz_model_io* io, int32_t precision, void* stream);
 /* The autotuner: for every component count present, time the group's staged
  * sequence on a strided sample of its points (up to sample_points) for each
- * candidate launch shape and keep the fastest (the next nz_models_flash
- * captures a new graph).  Synchronises the stream. */
+ * candidate launch shape and keep the fastest; the groups are timed side by
+ * side on their own streams, as they run in the graph (the next
+ * nz_models_flash captures a new graph).  Synchronises the stream. */
 int nz_models_tune(nz_models* m, const nz_model_io* io, int32_t precision,
                    int64_t sample_points, void* stream);
 /* Launch shape of a component count: resident blocks per SM of the lane

@@ -579,65 +579,85 @@ extern "C" int nz_models_tune(nz_models *m, const nz_model_io *io, int32_t preci
     if (e != cudaSuccess)
         return cudaFail(e, "nz_models_tune: set-up");
     const bool mixed = precision == NZ_PRECISION_MIXED;
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
-    for (size_t gi = 0; gi < m->groups.size() && rc == NZ_OK; ++gi)
+    const size_t ng = m->groups.size();
+    std::vector<cudaEvent_t> t0(ng), t1(ng);
+    for (size_t g = 0; g < ng; ++g)
+    {
+        cudaEventCreate(&t0[g]);
+        cudaEventCreate(&t1[g]);
+    }
+    std::vector<int64_t> count(ng);
+    for (size_t gi = 0; gi < ng; ++gi)
     {
         ModelGroup &g = m->groups[gi];
-        const int64_t count = std::min(g.points, sample_points);
-        const int64_t step = std::max<int64_t>(1, g.points / count);
-        const ModelPtrs *table = m->devTable + g.tableOffset;
-        modelsGatherKernel<<<gridFor(count, m->smCount), kModelsBlock, 0, g.stream>>>(
-            count, step, g.nc, g.pmodel, g.plocal, table, g.P, g.T, g.z, g.sal, g.model);
-        auto timeShape = [&](int lane, int warp, float &ms) {
-            g.laneBlocksPerSm = lane;
-            g.warpBlocksPerSm = warp;
-            cudaEventRecord(t0, g.stream);
-            const int r = launchGroup(m, int(gi), count, mixed);
-            cudaEventRecord(t1, g.stream);
-            const cudaError_t se = cudaEventSynchronize(t1);
+        count[gi] = std::min(g.points, sample_points);
+        const int64_t step = std::max<int64_t>(1, g.points / count[gi]);
+        modelsGatherKernel<<<gridFor(count[gi], m->smCount), kModelsBlock, 0, g.stream>>>(
+            count[gi], step, g.nc, g.pmodel, g.plocal, m->devTable + g.tableOffset, g.P, g.T, g.z, g.sal, g.model);
+    }
+    // One candidate shape per group, all groups at once on their own streams
+    // (as they run in the graph); each group's time from its own events.
+    auto timeAll = [&](const std::vector<int> &lane, const std::vector<int> &warp, std::vector<float> &ms) {
+        for (size_t gi = 0; gi < ng; ++gi)
+        {
+            ModelGroup &g = m->groups[gi];
+            g.laneBlocksPerSm = lane[gi];
+            g.warpBlocksPerSm = warp[gi];
+            cudaEventRecord(t0[gi], g.stream);
+            const int r = launchGroup(m, int(gi), count[gi], mixed);
+            cudaEventRecord(t1[gi], g.stream);
             if (r)
                 return r;
+        }
+        for (size_t gi = 0; gi < ng; ++gi)
+        {
+            const cudaError_t se = cudaEventSynchronize(t1[gi]);
             if (se != cudaSuccess)
                 return cudaFail(se, "nz_models_tune: sample run");
-            cudaEventElapsedTime(&ms, t0, t1);
-            return int(NZ_OK);
-        };
-        // coordinate search: lane-kernel blocks at the default warp shape,
-        // then warp-kernel blocks at the best lane shape (one untimed warm run)
-        float ms = 0.0f, best = 0.0f;
-        rc = timeShape(kTrialBlocksPerSm, 8, ms);
-        int bestLane = kTrialBlocksPerSm, bestWarp = 8;
-        bool first = true;
-        for (int lane : {2, 4, 8, 16})
-        {
-            if (rc)
-                break;
-            rc = timeShape(lane, 8, ms);
-            if (!rc && (first || ms < best))
-            {
-                best = ms;
-                bestLane = lane;
-                first = false;
-            }
+            cudaEventElapsedTime(&ms[gi], t0[gi], t1[gi]);
         }
-        for (int warp : {4, 16})
-        {
-            if (rc)
-                break;
-            rc = timeShape(bestLane, warp, ms);
-            if (!rc && ms < best)
+        return int(NZ_OK);
+    };
+    // coordinate search: lane-kernel blocks at the default warp shape, then
+    // warp-kernel blocks at each group's best lane shape (one untimed warm run)
+    std::vector<int> lane(ng, kTrialBlocksPerSm), warp(ng, 8), bestLane(ng, kTrialBlocksPerSm), bestWarp(ng, 8);
+    std::vector<float> ms(ng, 0.0f), best(ng, 0.0f);
+    rc = timeAll(lane, warp, ms);
+    bool first = true;
+    for (int l : {2, 4, 8, 16})
+    {
+        if (rc)
+            break;
+        std::fill(lane.begin(), lane.end(), l);
+        rc = timeAll(lane, warp, ms);
+        for (size_t gi = 0; gi < ng && !rc; ++gi)
+            if (first || ms[gi] < best[gi])
             {
-                best = ms;
-                bestWarp = warp;
+                best[gi] = ms[gi];
+                bestLane[gi] = l;
             }
-        }
-        g.laneBlocksPerSm = bestLane;
-        g.warpBlocksPerSm = bestWarp;
+        first = false;
     }
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+    for (int w : {4, 16})
+    {
+        if (rc)
+            break;
+        std::fill(warp.begin(), warp.end(), w);
+        rc = timeAll(bestLane, warp, ms);
+        for (size_t gi = 0; gi < ng && !rc; ++gi)
+            if (ms[gi] < best[gi])
+            {
+                best[gi] = ms[gi];
+                bestWarp[gi] = w;
+            }
+    }
+    for (size_t gi = 0; gi < ng; ++gi)
+    {
+        m->groups[gi].laneBlocksPerSm = bestLane[gi];
+        m->groups[gi].warpBlocksPerSm = bestWarp[gi];
+        cudaEventDestroy(t0[gi]);
+        cudaEventDestroy(t1[gi]);
+    }
     m->dropGraph();
     return rc;
 }
