@@ -622,6 +622,45 @@ NZ_HD void trialInit(Solver<NC> &s, TrialLane<NC> &L, const double *seedIn)
     L.mode = ssiSteps > 0 ? TM_SSI : (s.O().stabilityNewton > 0 ? TM_NEWTON : TM_TAIL);
 }
 
+// The mixed form's FP32 phase of a trial (run ahead of the FP64 steps, in its
+// own kernel): leading SSI steps with FP32 mixing and ln phi (FP64 root),
+// which never end a trial, until the FP32 residual is below
+// kMixedSsiHandover, the leading budget is spent, or an FP32 evaluation
+// fails; every later step is FP64.  Returns -1 when the trial ended invalid
+// (an empty trailing budget), else 0 with L ready for the FP64 steps.
+template <int NC>
+NZ_HD bool trialEnterTail(Solver<NC> &s, TrialLane<NC> &L);
+
+template <int NC>
+NZ_HD int trialMixedPhase(Solver<NC> &s, TrialLane<NC> &L)
+{
+    const FlashOpts &O = s.O();
+    const int ssiSteps = imin(O.maxStability, imax(O.stabilitySsi, 0));
+    StabilityResidual<NC> r;
+    while (L.mode == TM_SSI && !L.fp64Ssi)
+    {
+        if (!s.stabilityResidualMixed(L.candidate, L.P, L.T, L.logRef, L.logW, r))
+            break;
+        for (int i = 0; i < NC; ++i)
+            L.logW[i] = L.logRef[i] - r.lnphi[i];
+        ++L.it;
+        if (L.it >= ssiSteps)
+        {
+            if (O.stabilityNewton > 0)
+            {
+                L.mode = TM_NEWTON;
+                L.it = 0;
+            }
+            else if (!trialEnterTail(s, L))
+                return -1;
+        }
+        else if (r.norm < kMixedSsiHandover)
+            L.fp64Ssi = true;
+    }
+    L.fp64Ssi = true;
+    return 0;
+}
+
 // Enter the trailing SSI budget; false when it is empty (trial invalid).
 template <int NC>
 NZ_HD bool trialEnterTail(Solver<NC> &s, TrialLane<NC> &L)
@@ -651,30 +690,6 @@ NZ_HD int trialStep(Solver<NC> &s, TrialLane<NC> &L, TrialOut<NC> &out)
     const bool probing = L.mode == TM_FD || L.mode == TM_LINE;
     const FlashOpts &O = s.O();
     const int ssiSteps = imin(O.maxStability, imax(O.stabilitySsi, 0));
-    // Mixed form: the leading SSI steps evaluate ln phi with FP32 mixing (FP64
-    // root) and never end a trial.  Once the FP32 residual is small the rest of
-    // the leading steps run in FP64 (where a trial may converge, as in the
-    // FP64 form); the Newton steps and the SSI tail are FP64 throughout.
-    if (L.mode == TM_SSI && s.mixed && !L.fp64Ssi &&
-        s.stabilityResidualMixed(L.candidate, L.P, L.T, L.logRef, L.logW, r))
-    {
-        for (int i = 0; i < NC; ++i)
-            L.logW[i] = L.logRef[i] - r.lnphi[i];
-        ++L.it;
-        if (L.it >= ssiSteps)
-        {
-            if (O.stabilityNewton > 0)
-            {
-                L.mode = TM_NEWTON;
-                L.it = 0;
-            }
-            else if (!trialEnterTail(s, L))
-                return -1;
-        }
-        else if (r.norm < kMixedSsiHandover)
-            L.fp64Ssi = true;
-        return 0;
-    }
     s.stabilityResidual(L.candidate, L.P, L.T, L.logRef, probing ? L.probe : L.logW, r);
     switch (L.mode)
     {

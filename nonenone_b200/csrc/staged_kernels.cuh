@@ -537,6 +537,75 @@ stagedThreeResumeKernel(const __grid_constant__ FluidDev F, const __grid_constan
 
 // Every (task, seed) TPD trial is a lane; idle lanes are refilled from the
 // round's task list with one atomic per warp.
+// A TrialOut slot holding a trial's state after the mixed form's FP32 phase
+// (x = ln W, sum = steps done, trivial = mode) rather than a result.
+constexpr int kTrialMixedContinue = 0x4d495844;
+
+// The mixed form's FP32 phase of every queued trial of this round, thread per
+// trial (trialMixedPhase: at most the leading SSI budget of
+// FP32 steps), ahead of stagedTrialKernel, which then runs every later step
+// in FP64 -- so the FP64 kernel carries no FP32 code.
+template <int NC>
+__global__ void __launch_bounds__(kTrialBlock)
+stagedTrialMixedKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int round)
+{
+    if (stagedTripped(a))
+        return;
+    const int q = round & 1;
+    const int nseeds = seedCount<NC>(F);
+    const int ntasks = a.counters[4 * round];
+    const long long total = static_cast<long long>(ntasks < 3 * a.n ? ntasks : 3 * a.n) * nseeds;
+    const DriverState<NC> *states = static_cast<const DriverState<NC> *>(a.states);
+    TrialOut<NC> *trials = static_cast<TrialOut<NC> *>(a.trials);
+    unsigned long long evals = 0;
+    Solver<NC> s;
+    TrialLane<NC> L;
+    for (long long idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x)
+    {
+        const unsigned long long task = a.tasks[q][idx / nseeds];
+        const int seedIndex = int(idx % nseeds);
+        const int64_t point = int64_t(task >> 2);
+        const int cand = int(task & 3u);
+        if (point < 0 || point >= a.n || cand > 2)
+            continue;   // the trial kernel reports it
+        const DriverState<NC> &st = states[point];
+        s.setup(pointFluid(F, a, point), st.sal);
+        s.mixed = true;
+        L.P = st.P;
+        L.T = st.T;
+        L.candidate = cand;
+        for (int c = 0; c < NC; ++c)
+        {
+            L.logRef[c] = st.logRef[c];
+            L.ref[c] = st.refX[c];
+        }
+        double seed[NC];
+        s.stabilitySeed(seedIndex, st.P, st.T, st.z, st.refX, seed);
+        trialInit<NC>(s, L, seed);
+        const int rc = trialMixedPhase<NC>(s, L);
+        TrialOut<NC> &o = trials[(point * 3 + cand) * nseeds + seedIndex];
+        if (rc != 0 || s.err)
+        {
+            o.valid = s.err ? -s.err : 0;
+            o.trivial = 0;
+            o.sum = 0.0;
+            for (int c = 0; c < NC; ++c)
+                o.x[c] = 0.0;
+        }
+        else
+        {
+            o.valid = kTrialMixedContinue;
+            o.trivial = L.mode;
+            o.sum = double(L.it);
+            for (int c = 0; c < NC; ++c)
+                o.x[c] = L.logW[c];
+        }
+        evals += s.evals;
+    }
+    warpAddEvals(a.evalCounter, evals);
+}
+
 template <int NC>
 __global__ void __launch_bounds__(kTrialBlock)
 stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int round)
@@ -592,7 +661,6 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                     const DriverState<NC> &st = states[bad ? 0 : point];
                     evals += s.evals;
                     s.setup(pointFluid(F, a, bad ? 0 : point), st.sal);
-                    s.mixed = a.mixed != 0;
                     L.P = st.P;
                     L.T = st.T;
                     L.candidate = cand;
@@ -605,6 +673,22 @@ stagedTrialKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
                     s.stabilitySeed(seedIndex, st.P, st.T, st.z, st.refX, seed);
                     trialInit<NC>(s, L, seed);
                     slot = bad ? -2 : (point * 3 + cand) * nseeds + seedIndex;
+                    if (a.mixed && !bad)
+                    {
+                        // the mixed form's FP32 phase ran ahead (stagedTrialMixedKernel):
+                        // continue from its state, or leave a trial it ended
+                        const TrialOut<NC> &pre = trials[slot];
+                        if (pre.valid == kTrialMixedContinue)
+                        {
+                            for (int c = 0; c < NC; ++c)
+                                L.logW[c] = pre.x[c];
+                            L.it = int(pre.sum);
+                            L.mode = pre.trivial;
+                            L.fp64Ssi = true;
+                        }
+                        else
+                            slot = -1;
+                    }
                 }
                 else
                 {
@@ -1509,6 +1593,8 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
     const unsigned trialGrid = unsigned(smCount * tune.laneBlocksPerSm);
     for (int round = 0; round + 1 < kMaxRounds; ++round)
     {
+        if (mixed)
+            stagedTrialMixedKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a, round);
         stagedTrialKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a, round);
         if (after("trial", round))
             return setError(NZ_ERR_CUDA, "staged flash self-check failed in trials");
@@ -1531,6 +1617,8 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in recovery");
     for (int rr = 0; rr < kRecoveryRounds; ++rr)
     {
+        if (mixed)
+            stagedTrialMixedKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a, kMaxRounds + rr);
         stagedTrialKernel<NC><<<trialGrid, kTrialBlock, 0, st>>>(F, a, kMaxRounds + rr);
         stagedRecoverResumeKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out, rr);
         if (after("recover round", kMaxRounds + rr + 1))
