@@ -236,9 +236,9 @@ int nz_ctx_set_spin_limit(nz_ctx* ctx, int64_t limit);
  * whether it has a water component, which adds a stability seed, and whether
  * it is Soreide-Whitson, which adds the allocation-search memos); the error
  * message states the exact limit for the context's fluid.  For PR / PR-CPA
- * fluids with a water component it is 13,751 points for nc = 3, 7,601 for
- * nc = 6 and 5,620 for nc = 8; for Soreide-Whitson fluids 10,666 / 5,975 /
- * 4,431.  The first call on a
+ * fluids with a water component it is 13,980 points for nc = 3, 7,712 for
+ * nc = 6 and 5,696 for nc = 8; for Soreide-Whitson fluids 10,808 / 6,047 /
+ * 4,480.  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress) and
  * should therefore come before any stream capture.  All calls share the one
  * array and the context's evaluation counter: calls that overlap on the GPU

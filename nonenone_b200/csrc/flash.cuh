@@ -1120,82 +1120,17 @@ struct Solver
     NZ_HDN void flashTwo(double P, double T, const double *z, int first, int second,
                                           const double *Kin, Result<NC> &r)
     {
-        double K[NC];
-#pragma unroll
-        for (int i = 0; i < NC; ++i)
-            K[i] = sclamp(Kin[i], 1.0e-100, 1.0e100);
-        flashTwoFrom(P, T, z, first, second, K, 0.5, 0, r);
-    }
-
-    // The mixed form's FP32 successive-substitution step of flashTwo: RR2 in
-    // FP64, the two phases' ln phi with FP32 mixing (FP64 root), the K update
-    // of twoSsiStep.  It never ends a solve; false when the step cannot be
-    // taken in FP32 (K and betaSecond are then unchanged).  `residual` is the
-    // step's largest |d ln K|.
-    NZ_HDN bool twoSsiStepMixed(double P, double T, const double *z, int first, int second, double *K,
-                                double &betaSecond, double &residual)
-    {
-        if (F->eosModel == EOS_CPA)
-            return false;
-        double bS;
-        if (!rr2(z, K, betaSecond, bS))
-            return false;
-        double a[NC], b[NC];
-#pragma unroll
-        for (int i = 0; i < NC; ++i)
-        {
-            const double D = (1.0 - bS) + bS * K[i];
-            if (!(D > 0.0) || !isfinite(D))
-                return false;
-            a[i] = z[i] / D;
-            b[i] = K[i] * a[i];
-        }
-        normalize(a);
-        normalize(b);
-        if (err)
-            return false;
-        const int ra = thermodynamicRole(first), rb = thermodynamicRole(second);
-        ensureCache(P, T);
-        double la[NC], lb[NC];
-        if (!lnPhiMixed<NC>(a, (ra == WATER && sw()) ? aq : nonAq, F->m1, F->m2, ra == GAS, la) ||
-            !lnPhiMixed<NC>(b, (rb == WATER && sw()) ? aq : nonAq, F->m1, F->m2, rb == GAS, lb))
-            return false;
-        evals += 2;
-        double next[NC];
-        double maxResidual = 0.0;
-#pragma unroll
-        for (int i = 0; i < NC; ++i)
-        {
-            const double d = sclamp(la[i] - lb[i] - log(K[i]), -O().logKLimit, O().logKLimit);
-            if (!isfinite(d))
-                return false;
-            maxResidual = smax(maxResidual, fabs(d));
-            next[i] = sclamp(K[i] * exp(0.6 * d), 1.0e-100, 1.0e100);
-        }
-#pragma unroll
-        for (int i = 0; i < NC; ++i)
-            K[i] = next[i];
-        betaSecond = bS;
-        residual = maxResidual;
-        return true;
-    }
-
-    // flashTwo from a given state: K (already clamped), the second phase's
-    // fraction guess, and `stepsDone` leading SSI steps already taken (the
-    // mixed form's FP32 steps; 0 for flashTwo itself).
-    NZ_HDN void flashTwoFrom(double P, double T, const double *z, int first, int second, const double *Kin,
-                             double betaSecond, int stepsDone, Result<NC> &r)
-    {
         r.init();
         r.presence = uint8_t(bitOf(first) | bitOf(second));
         double K[NC];
 #pragma unroll
         for (int i = 0; i < NC; ++i)
-            K[i] = Kin[i];
-        int total = stepsDone;
+            K[i] = sclamp(Kin[i], 1.0e-100, 1.0e100);
+        double betaSecond = 0.5;
+        int total = 0;
         const int ssiSteps = imin(O().maxIterations, imax(O().twoSsi, 0));
 #pragma unroll 1
-        for (int it = stepsDone; it < ssiSteps; ++it)
+        for (int it = 0; it < ssiSteps; ++it)
         {
             if (!twoSsiStep(P, T, z, first, second, K, betaSecond, total, r))
                 return;

@@ -60,10 +60,6 @@ struct DriverState
     double threeKg[NC];   // starting K of the pending three-phase solve
     double threeKw[NC];
     int allocSlot;        // SW allocation search precomputed in this memo slot (-1: none)
-    // mixed form: the seed flashTwo's state after its FP32 steps
-    double seedK[NC];
-    double seedBeta;
-    int seedSteps;
 };
 
 template <int NC>
@@ -536,10 +532,8 @@ struct Driver
         return STAGE_NEED_FULL;
     }
 
-    // flash() up to the active-set loop (three_phase_flash.hpp:87-104).  With
-    // `afterFp32`, the seed flashTwo continues from the mixed form's FP32
-    // steps kept in the state (seedK, seedBeta, seedSteps).
-    NZ_HD uint8_t start(double P, double T, const double *zIn, bool afterFp32 = false)
+    // flash() up to the active-set loop (three_phase_flash.hpp:87-104).
+    NZ_HD uint8_t start(double P, double T, const double *zIn)
     {
         st->P = P;
         st->T = T;
@@ -556,10 +550,7 @@ struct Driver
         double kg[NC];
         s.wilsonK(P, T, kg);
         Result<NC> &seed = st->seed;
-        if (afterFp32)
-            s.flashTwoFrom(P, T, st->z, OIL, GAS, st->seedK, st->seedBeta, st->seedSteps, seed);
-        else
-            s.flashTwo(P, T, st->z, OIL, GAS, kg, seed);
+        s.flashTwo(P, T, st->z, OIL, GAS, kg, seed);
         uint8_t active = s.presenceFromFractions(seed.beta);
         if (!seed.converged || active == 0)
         {

@@ -248,65 +248,11 @@ stagedStartKernel(const __grid_constant__ FluidDev F, const __grid_constant__ St
         double zi[NC];
         for (int c = 0; c < NC; ++c)
             zi[c] = a.z[c * a.n + i];
-        uint8_t stage = d.start(a.P[i], a.T[i], zi, a.mixed != 0);
+        uint8_t stage = d.start(a.P[i], a.T[i], zi);
         if (stage == STAGE_DONE)
             stage = d.activeSetLoop(false, nullptr);
         routePoint<NC>(a, out, 0, i, stage, d);
         evals = d.s.evals;
-    }
-    warpAddEvals(a.evalCounter, evals);
-}
-
-// The mixed form's FP32 steps of every point's seed flashTwo(Oil, Gas) from
-// Wilson K, thread per point, ahead of the start kernel: leading SSI steps
-// with FP32 ln phi (Solver::twoSsiStepMixed) until the step's |d ln K| is
-// below kMixedSsiHandover, the leading budget is spent or a step cannot be
-// taken in FP32; the start kernel continues the solve from there in FP64.
-template <int NC>
-__global__ void __launch_bounds__(kFlashBlock)
-stagedSeedMixedKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
-{
-    if (stagedTripped(a))
-        return;
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    unsigned long long evals = 0;
-    if (i < a.n)
-    {
-        DriverState<NC> &st = static_cast<DriverState<NC> *>(a.states)[i];
-        Solver<NC> s;
-        s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
-        const double P = a.P[i], T = a.T[i];
-        double zn[NC], K[NC];
-        for (int c = 0; c < NC; ++c)
-        {
-            zn[c] = a.z[c * a.n + i];
-            K[c] = 1.0;
-        }
-        double beta = 0.5;
-        int steps = 0;
-        if (s.validatePT(P, T))
-        {
-            s.normalize(zn);
-            double kg[NC];
-            s.wilsonK(P, T, kg);
-            for (int c = 0; c < NC; ++c)
-                K[c] = sclamp(kg[c], 1.0e-100, 1.0e100);
-            const int ssiSteps = imin(s.O().maxIterations, imax(s.O().twoSsi, 0));
-            while (!s.err && steps < ssiSteps)
-            {
-                double residual = 0.0;
-                if (!s.twoSsiStepMixed(P, T, zn, OIL, GAS, K, beta, residual))
-                    break;
-                ++steps;
-                if (residual < kMixedSsiHandover)
-                    break;
-            }
-        }
-        for (int c = 0; c < NC; ++c)
-            st.seedK[c] = K[c];
-        st.seedBeta = beta;
-        st.seedSteps = steps;
-        evals = s.evals;
     }
     warpAddEvals(a.evalCounter, evals);
 }
@@ -1641,8 +1587,6 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         return e == cudaSuccess && c[kCounterBound] == 0 && c[kCounterGuard] == 0 ? 0 : -1;
     };
     const unsigned gridN = unsigned((n + kFlashBlock - 1) / kFlashBlock);
-    if (mixed)
-        stagedSeedMixedKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a);
     stagedStartKernel<NC><<<gridN, kFlashBlock, 0, st>>>(F, a, out);
     if (after("start", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed after start");

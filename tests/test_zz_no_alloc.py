@@ -85,4 +85,4 @@ def test_noalloc_refuses_batches_beyond_its_work_space(golden):
     msg = fl.lib.nz_last_error()
     assert b"work space" in msg
     # the limit the header documents for nc = 3 with a water component
-    assert b"at most 13751 points for nc=3" in msg, msg
+    assert b"at most 13980 points for nc=3" in msg, msg
