@@ -284,7 +284,7 @@ def natural_measure(local: int, reps: int, hbm_peak: float | None, with_cpu: boo
     return results
 
 
-def serving_measure(local: int, n_requests: int, rate: float = 20.0):
+def serving_measure(local: int, n_requests: int, rate: float = 20.0, slots: int = 4):
     """The request loop (nonenone_b200.serving) over a Poisson stream: each
     request one flash + assembly job (new model: per-cell P-T-z flash, history,
     residual, BAIJ Jacobian; repeat iteration of a resident model, 30 %:
@@ -294,13 +294,13 @@ def serving_measure(local: int, n_requests: int, rate: float = 20.0):
     run of PR-CPA and SW initialisations stays within the bench's minutes)."""
     from nonenone_b200 import serving
     reqs = serving.poisson_requests(n_requests, rate=rate, seed=5, cells=(1.0e3, 1.0e4))
-    ex = serving.NaturalExecutor(device=local, slots=4)
+    ex = serving.NaturalExecutor(device=local, slots=slots)
     # build the fluids' contexts before the clock starts
     for r in reqs:
         ex._context(r.nc, r.eos, 0)
-    out = serving.ServingLoop(ex, slots=4, hbm_budget=150.0e9).run(reqs)
+    out = serving.ServingLoop(ex, slots=slots, hbm_budget=150.0e9).run(reqs)
     stats = serving.summarize(out)
-    stats.update({"arrival_rate_req_per_s": rate, "slots": 4, "hbm_budget_bytes": 150.0e9,
+    stats.update({"arrival_rate_req_per_s": rate, "slots": slots, "hbm_budget_bytes": 150.0e9,
                   "cells": "log-uniform [1e3, 1e4]", "repeat_fraction": 0.3,
                   "errors": [o.error for o in out if o.error][:3]})
     return stats
@@ -780,7 +780,7 @@ def run_gpu(args):
 
     serving_stats = None
     if rank == 0 and args.serving_requests > 0:
-        serving_stats = serving_measure(local, args.serving_requests)
+        serving_stats = serving_measure(local, args.serving_requests, slots=args.serving_slots)
 
     multi_model = None
     if rank == 0 and args.models > 0:
@@ -817,6 +817,12 @@ def run_gpu(args):
                        "points_per_batch": N_POINTS, "eos": "PR", "nc": NC,
                        "precision": headline, "batches_in_flight": M,
                        "near_boundary_points": nb,
+                       "mixture": ("95 % a label-free proposal mixture drawn to ~40/40/20 % single/two/three-phase "
+                                   "by the reference label: 45 % z_H2O ~ U[0, 5e-4] with (CO2, nC10) ~ Dir(1, 1) "
+                                   "in the box's P/T; 32 % the box itself (P ~ U[5, 40] MPa, T ~ U[303, 423] K, "
+                                   "z ~ Dir(2, 1, 1)); 23 % a three-phase proposal outside the box's z law "
+                                   "(P ~ U[5, 12] MPa, T ~ U[340, 423] K, z ~ Dir(2, 2, 0.6)); + 5 % within "
+                                   "5e-6 relative of a pressure where a phase appears"),
                        "l2": f"not flushed: {M} distinct input sets of 42 MB and output sets of "
                              f"{d2h / 1e6:.0f} MB per batch in flight exceed the 126 MB L2",
                        "label_mix": {"single": float(np.isin(presence, [1, 2, 4]).mean()),
@@ -881,6 +887,8 @@ def main():
                     help="skip the Natural Newton-evaluation measurements")
     ap.add_argument("--serving-requests", type=int, default=24,
                     help="requests of the serving-loop measurement (0 skips it)")
+    ap.add_argument("--serving-slots", type=int, default=4,
+                    help="concurrent request slots of the serving loop")
     ap.add_argument("--models", type=int, default=32,
                     help="models of the uneven multi-model batch measurement (0 skips it)")
     ap.add_argument("--model-cells", default="100,1000",
