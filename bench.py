@@ -887,7 +887,7 @@ def main():
                     help="skip the Natural Newton-evaluation measurements")
     ap.add_argument("--serving-requests", type=int, default=24,
                     help="requests of the serving-loop measurement (0 skips it)")
-    ap.add_argument("--serving-slots", type=int, default=4,
+    ap.add_argument("--serving-slots", type=int, default=8,
                     help="concurrent request slots of the serving loop")
     ap.add_argument("--models", type=int, default=32,
                     help="models of the uneven multi-model batch measurement (0 skips it)")
