@@ -541,13 +541,13 @@ def staged_launches(precision_name: str, sw: bool = False) -> int:
     """Kernels one batch launches: the plain FP64 form one; the staged forms
     start, 8 rounds x 8, recovery 1 (5), recovery 2 (3 x 2), the recovery
     kernel (SW: the allocation queue and seed kernels, then the recovery
-    kernel in two passes around the role-permutation kernel), 8
-    continuation-anchor launches, select and check (+ for the mixed form its
+    kernel in two passes around the role-permutation kernel), the
+    continuation anchors, select and check (+ for the mixed form its
     FP32 trial phase before each of the 11 trial launches, and the polish)."""
     if precision_name == "fp64":
         return 1
     recovery = 5 if sw else 1
-    return 1 + 8 * 8 + 5 + 3 * 2 + recovery + 8 + 1 + 1 + (12 if precision_name == "mixed" else 0)
+    return 1 + 8 * 8 + 5 + 3 * 2 + recovery + 1 + 1 + 1 + (12 if precision_name == "mixed" else 0)
 
 
 def form_error(out, ref_out):

@@ -1286,13 +1286,14 @@ stagedFullKernel(const __grid_constant__ FluidDev F, const __grid_constant__ Sta
     warpAddEvals(a.evalCounter, evals);
 }
 
-// Pressure-continuation anchors of the queued points: one warp per (point,
-// anchor), the lanes splitting the stability seeds as in the recovery kernel.
-// Launched once per anchor, for the points the earlier anchors left undecided.
+// Pressure-continuation anchors as each queued point's own chain: one warp per
+// point runs its anchors in the fallback's order and stops at the first one
+// with an outcome (the lanes splitting the stability seeds as in the recovery
+// kernel) -- the fallback's own work, and no point waits for another's
+// anchor before starting its next.
 template <int NC>
 __global__ void __launch_bounds__(kFlashBlock)
-stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a, int first,
-                   int span)
+stagedAnchorChainKernel(const __grid_constant__ FluidDev F, const __grid_constant__ StagedArgs a)
 {
     if (stagedTripped(a))
         return;
@@ -1303,15 +1304,8 @@ stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
     const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
     AnchorOut<NC> *anchors = static_cast<AnchorOut<NC> *>(a.anchors);
     unsigned long long evals = 0;
-    for (int64_t t = warpId; t < count * span; t += nwarps)
+    for (int64_t k = warpId; k < count; k += nwarps)
     {
-        const int64_t k = t / span;
-        const int an = first + int(t % span);
-        bool decided = false;
-        for (int earlier = 0; earlier < first; ++earlier)
-            decided = decided || anchors[k * kAnchors + earlier].outcome != CONT_NONE;
-        if (decided)
-            continue;   // an earlier anchor has an outcome: it decides the point
         const int64_t i = a.cont[k];
         if (i < 0 || i >= a.n)
         {
@@ -1319,24 +1313,31 @@ stagedAnchorKernel(const __grid_constant__ FluidDev F, const __grid_constant__ S
                 atomicExch(&a.counters[kCounterBound], 8);
             continue;
         }
-        Solver<NC> s;
-        s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
-        s.lane = lane;
-        s.width = 32;
         double zn[NC];
-        for (int c = 0; c < NC; ++c)
-            zn[c] = a.z[c * a.n + i];
-        s.normalize(zn);
-        Result<NC> r;
-        const int outcome = s.continuationAnchor(a.P[i], a.T[i], zn, an, r);
-        if (lane == 0)
+#pragma unroll 1
+        for (int an = 0; an < kAnchors; ++an)
         {
-            AnchorOut<NC> &o = anchors[k * kAnchors + an];
-            o.outcome = outcome;
-            o.err = s.err;
-            if (outcome == CONT_SUCCESS)
-                o.r = r;
-            evals += s.evals;
+            Solver<NC> s;
+            s.setup(pointFluid(F, a, i), pointSalinity(F, a, i));
+            s.lane = lane;
+            s.width = 32;
+            for (int c = 0; c < NC; ++c)
+                zn[c] = a.z[c * a.n + i];
+            s.normalize(zn);
+            Result<NC> r;
+            const int outcome = s.continuationAnchor(a.P[i], a.T[i], zn, an, r);
+            __syncwarp();
+            if (lane == 0)
+            {
+                AnchorOut<NC> &o = anchors[k * kAnchors + an];
+                o.outcome = outcome;
+                o.err = s.err;
+                if (outcome == CONT_SUCCESS)
+                    o.r = r;
+                evals += s.evals;
+            }
+            if (outcome != CONT_NONE)
+                break;
         }
     }
     warpAddEvals(a.evalCounter, evals);
@@ -1636,11 +1637,9 @@ int stagedLaunch(const FluidDev &F, void *scratch, int64_t n, const double *P, c
         stagedFullKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, out, 0);
     if (after("full", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the full solver");
-    // one launch per anchor, each for the points no earlier anchor decided:
-    // the work is the fallback's own (it stops at the first anchor with an
-    // outcome), the points run side by side
-    for (int an = 0; an < kAnchors; ++an)
-        stagedAnchorKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a, an, 1);
+    // each queued point's anchors as one warp's chain: the fallback's own
+    // work, and the launch lasts as long as the longest chain
+    stagedAnchorChainKernel<NC><<<warpGrid, kFlashBlock, 0, st>>>(F, a);
     stagedSelectKernel<NC><<<unsigned(smCount * 2), kFlashBlock, 0, st>>>(F, a, out);
     if (after("continuation", 0))
         return setError(NZ_ERR_CUDA, "staged flash self-check failed in the pressure continuation");
